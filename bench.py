@@ -1,0 +1,374 @@
+#!/usr/bin/env python
+"""Benchmark of the Elastic2D time-stepping path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+One step is one complete shot of the workload: the 4444 x 3819 layered
+medium, 8th order, nbc 50, free surface, nt = 11520 (the shape of the
+reference's only published timing, README.md:93-102).  Metric: Gcell-steps/s
+over padded cells (4552 x 3927) x nt, whole job (all ranks).
+
+Multi-GPU: one process per GPU (torchrun); shots are independent, so every
+rank runs its own shot with no data-path collective (weak scaling).  The
+timed region is bracketed by a barrier and a device synchronisation and
+timed with CUDA events on the library's stream; the max over ranks is taken.
+
+``--impl reference`` times the CPU restatement of the reference (the
+oracle/ port; Julia is not available) on the host cores, rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+PUBLISHED_CUDA_GCELLS = 1.14   # README.md:102: < 3 min on an RTX 3060 -> > 1.14 Gcell-steps/s
+METRIC = "Gcell-steps/s"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=3)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    p.add_argument("--nt", type=int, default=None, help="override nt (development only: not the workload)")
+    p.add_argument("--profile-steps", type=int, default=200)
+    p.add_argument("--cpu-seconds", type=float, default=15.0)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-e2e", action="store_true")
+    return p.parse_args()
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits", "-lms", "200",
+                 "-i", str(self.device)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        self.out = ""
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.out, _ = self.proc.communicate(timeout=10)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                self.out, _ = self.proc.communicate()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in (self.out or "").splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------- workload
+def make_workload(nt_override):
+    from fomo_julia_b200 import synthetic
+    return synthetic.large_layered(seed=1, nt=nt_override)
+
+
+def host_inputs(w):
+    """Host-side set-up exactly as the reference's init.jl does it."""
+    import fomo_julia_b200 as F
+    pad = w.nbc + w.fd_order // 2
+    lam, mu, mu_txz, rho_vx, rho_vz = F.compute_staggered_params(
+        F.pad_array(w.vp, pad), F.pad_array(w.vs, pad), F.pad_array(w.rho, pad))
+    nx, nz = w.nx_in + 2 * pad, w.nz_in + 2 * pad
+    v_ref = F.julia_mean(w.vp) if w.vp.size <= 4_000_000 else np.float32(w.vp.mean(dtype=np.float64))
+    habc = F.init_habc(nx, nz, w.nbc, w.dt, w.dx, w.dz, v_ref)
+    params = F.sim_params(w.dt, w.nt, w.dx, w.dz, w.fd_order)
+    a = F.get_fd_coefficients(w.fd_order)
+    wav = F.ricker_wavelet(w.f0, w.dt, w.nt)
+    si = F.coord_to_index(w.src_x[0], w.dx, pad)
+    sj = F.coord_to_index(w.src_z[0], w.dz, pad)
+    ri = np.rint(w.rec_x.astype(np.float32) / np.float32(w.dx)).astype(np.int32) + pad + 1
+    rj = np.rint(w.rec_z.astype(np.float32) / np.float32(w.dz)).astype(np.int32) + pad + 1
+    return dict(pad=pad, nx=nx, nz=nz, arrays=(rho_vx, rho_vz, lam, mu, mu_txz), habc=habc, params=params,
+                a=a, wav=wav, si=si, sj=sj, ri=ri, rj=rj)
+
+
+# ---------------------------------------------------------------- reference arm
+def cpu_sample(w, hi, seconds: float, threads: int = 0):
+    """Times the oracle (CPU restatement of the reference) on the first time
+    steps of the same shot; returns (Gcell-steps/s, steps, cores)."""
+    import oracle
+    oracle.build()
+    med = oracle.OMedium(hi["nx"], hi["nz"], w.fd_order // 2, hi["pad"], w.nbc, w.dx, w.dz, w.free_surface,
+                         *hi["arrays"])
+    h = oracle.OHabc(w.nbc, np.array([hi["habc"].qx, hi["habc"].qz, hi["habc"].qt_x, hi["habc"].qt_z,
+                                      hi["habc"].qxt], dtype=np.float32),
+                     hi["habc"].w_vx, hi["habc"].w_vz, hi["habc"].w_tau)
+    cells = hi["nx"] * hi["nz"]
+
+    def run(n):
+        t = time.perf_counter()
+        oracle.run_shot(med, h, hi["a"], w.dt, w.nt, hi["si"], hi["sj"], hi["wav"], hi["ri"], hi["rj"], "vz",
+                        "simd8", n_steps=n, n_threads=threads)
+        return time.perf_counter() - t
+
+    t1 = run(2)
+    n = max(2, min(w.nt, int(seconds / max(t1 / 2, 1e-6))))
+    t = run(n)
+    cores = threads or oracle.max_threads()
+    return cells * n / t / 1e9, n, cores, t
+
+
+def reference_arm(args, rank, world):
+    if rank != 0:
+        return
+    w = make_workload(args.nt)
+    hi = host_inputs(w)
+    import oracle
+    oracle.build()
+    per_step_s = args.cpu_seconds / 2
+    vals = []
+    for k in range(args.warmup + args.steps):
+        v, n, cores, t = cpu_sample(w, hi, per_step_s)
+        if k >= args.warmup:
+            vals.append((v, n, t))
+    value = float(np.mean([v for v, _, _ in vals]))
+    n = vals[-1][1]
+    line = {
+        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": float(np.mean([t for _, _, t in vals]) * 1e3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "impl": "reference",
+        "config": {"workload": w.name, "cells_padded": hi["nx"] * hi["nz"], "nt": w.nt,
+                   "step": f"first {n} time steps of the shot (bounded CPU sample)"},
+        "cpu_baseline": {"value": value, "unit": METRIC, "cores": cores, "kind": "port",
+                         "sample": f"{n} time steps of {w.name} per step, OpenMP over {cores} threads "
+                                   f"(C++ restatement of the reference's Float32 CPU path; Julia absent)"},
+        "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------- B200 arm
+def b200_arm(args, rank, world, local):
+    import torch
+    import torch.distributed as dist
+    import fomo_julia_b200 as F
+    from fomo_julia_b200 import _lib
+    from fomo_julia_b200._lib import FomoKernelTime, FomoRunStats, call
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    _lib.ensure_init(local)
+    sp = ctypes.c_void_p(0)
+    call("fomo_b200_get_stream", ctypes.byref(sp))
+    stream = torch.cuda.ExternalStream(sp.value, device=torch.device("cuda", local))
+
+    w = make_workload(args.nt)
+    hi = host_inputs(w)
+    nx, nz = hi["nx"], hi["nz"]
+    cells = nx * nz
+    # pinned host copies of the inputs (medium arrays) and the output gather
+    pinned = []
+    for arr in hi["arrays"]:
+        t = torch.empty(arr.size, dtype=torch.float32, pin_memory=True)
+        t.numpy()[:] = np.asfortranarray(arr).ravel(order="F")
+        pinned.append(t)
+    n_rec = hi["ri"].size
+    gather = torch.zeros(w.nt * n_rec, dtype=torch.float32, pin_memory=True)
+
+    keep = []
+    H = F.elastic2d._ctypes_habc(hi["habc"], keep)
+    src = F.Source(hi["si"], hi["sj"], hi["wav"])
+    rec = F.Receivers(hi["ri"], hi["rj"], None, "vz")
+    S = F.elastic2d._ctypes_shot(hi["a"], hi["params"], src, rec, keep)
+
+    def medium_create():
+        h = ctypes.c_uint64(0)
+        call("fomo_b200_medium_create", nx, nz, w.fd_order // 2, hi["pad"], int(w.free_surface),
+             float(w.dx), float(w.dz), *[t.data_ptr() for t in pinned], ctypes.byref(h))
+        return h.value
+
+    med = medium_create()
+    wf = ctypes.c_uint64(0)
+    call("fomo_b200_wavefield_create", nx, nz, ctypes.byref(wf))
+    wf = wf.value
+
+    def device_shot():
+        """One shot with inputs resident: reset, nt steps, gather left on the device."""
+        sh = ctypes.c_uint64(0)
+        call("fomo_b200_shot_begin", med, wf, ctypes.byref(H), ctypes.byref(S), ctypes.byref(sh))
+        k = ctypes.c_int32(0)
+        call("fomo_b200_shot_advance", sh.value, w.nt, ctypes.byref(k))
+        st = FomoRunStats()
+        call("fomo_b200_shot_finish", sh.value, None, ctypes.byref(st))
+        return st
+
+    def e2e_shot():
+        """The drop-in call sequence with host buffers: upload the medium,
+        run the shot, read the gather back, release the medium."""
+        m2 = medium_create()
+        st = FomoRunStats()
+        call("fomo_b200_run_shot", m2, wf, ctypes.byref(H), ctypes.byref(S), gather.data_ptr(), ctypes.byref(st))
+        call("fomo_b200_medium_destroy", m2)
+        return st
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def timed(fn, k):
+        barrier()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        launches = 0
+        stats = []
+        for _ in range(k):
+            st = fn()
+            launches += st.kernel_launches
+            stats.append(st)
+        e1.record(stream)
+        e1.synchronize()
+        torch.cuda.synchronize()
+        barrier()
+        ms = e0.elapsed_time(e1)
+        if world > 1:
+            t = torch.tensor([ms], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms, launches, stats
+
+    for _ in range(args.warmup):
+        device_shot()
+    with ClockSampler(local) as clk:
+        ms, launches, _ = timed(device_shot, args.steps)
+    clocks = clk.summary()
+    value = world * args.steps * cells * w.nt / (ms / 1e3) / 1e9
+
+    e2e = None
+    if not args.no_e2e:
+        e2e_shot()
+        ms_e, _, st_e = timed(e2e_shot, args.steps)
+        h2d = sum(t.numel() * 4 for t in pinned) + st_e[0].h2d_bytes
+        e2e = {"value": world * args.steps * cells * w.nt / (ms_e / 1e3) / 1e9, "unit": METRIC,
+               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(st_e[0].d2h_bytes),
+               "ms_per_step": ms_e / args.steps,
+               "path": "fomo_b200_medium_create + fomo_b200_run_shot (pinned host buffers) + medium_destroy"}
+
+    # roofline of the dominant kernel: CUDA events around each launch
+    sh = ctypes.c_uint64(0)
+    call("fomo_b200_shot_begin", med, wf, ctypes.byref(H), ctypes.byref(S), ctypes.byref(sh))
+    kt = (FomoKernelTime * 8)()
+    nk = ctypes.c_int32(0)
+    call("fomo_b200_shot_profile", sh.value, min(args.profile_steps, w.nt), kt, 8, ctypes.byref(nk))
+    call("fomo_b200_shot_finish", sh.value, None, None)
+    kernels = []
+    for i in range(nk.value):
+        k = kt[i]
+        if k.launches:
+            avg = k.total_ms / k.launches
+            kernels.append({"name": k.name.decode(), "launches": k.launches, "avg_ms": avg,
+                            "bytes_per_launch": k.bytes_per_launch, "gbs": k.bytes_per_launch / (avg / 1e3) / 1e9})
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(REPO, "MEASURED_PEAKS.json")))
+        peak, peak_src = float(peaks["hbm_gbs"]), "measured"
+    except Exception:
+        peak, peak_src = 6650.0, "fallback"
+    dom = max(kernels, key=lambda k: k["avg_ms"] * k["launches"]) if kernels else None
+    step_ms = sum(k["avg_ms"] for k in kernels) if kernels else None
+    roofline = None
+    if dom:
+        traffic = None
+        tf = os.path.join(REPO, "profiles", "traffic.json")
+        if os.path.exists(tf):
+            traffic = json.load(open(tf)).get(dom["name"])
+        roofline = {"bound": "hbm", "kernel": dom["name"], "achieved": dom["gbs"], "peak": peak, "unit": "GB/s",
+                    "frac": dom["gbs"] / peak, "peak_source": f"{peak_src} (MEASURED_PEAKS.json hbm_gbs)",
+                    "traffic": traffic,
+                    "step_achieved": 60.0 * cells / (step_ms / 1e3) / 1e9 if step_ms else None,
+                    "step_frac": (60.0 * cells / (step_ms / 1e3) / 1e9) / peak if step_ms else None,
+                    "kernels": kernels}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        v, n, cores, t = cpu_sample(w, hi, args.cpu_seconds)
+        cpu = {"value": v, "unit": METRIC, "cores": cores, "kind": "port",
+               "sample": f"first {n} time steps of the same shot ({t:.1f} s), C++ restatement of the "
+                         f"reference's Float32 CPU path (oracle/), OpenMP"}
+
+    call("fomo_b200_wavefield_destroy", wf)
+    call("fomo_b200_medium_destroy", med)
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": value / PUBLISHED_CUDA_GCELLS, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": w.name, "cells_padded": cells, "grid_padded": [nx, nz], "nt": w.nt,
+                       "shots_per_gpu_per_step": 1, "parallelism": f"shot-sharded x{world}",
+                       "l2": "inputs larger than L2 (357 MB medium + 715 MB state per shot)",
+                       "bytes_per_cell_step_algorithmic": 60},
+            "e2e": e2e, "gpu_launches": int(launches), "clocks": clocks, "roofline": roofline,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    world, rank, local = dist_setup()
+    if args.impl == "reference":
+        reference_arm(args, rank, world)
+        return
+    b200_arm(args, rank, world, local)
+
+
+if __name__ == "__main__":
+    main()

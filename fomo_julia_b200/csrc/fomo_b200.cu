@@ -1,0 +1,675 @@
+// fomo_b200.cu -- host runtime and C ABI of libfomo_b200.so (include/fomo_b200.h).
+//
+// Owns every device allocation behind opaque handles, one CUDA stream per
+// process, and the time loop of a shot.  See include/fomo_b200.h for the
+// reference interface each entry point stands in for.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/fomo_b200.h"
+#include "step_simple.cuh"
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return code;
+}
+
+#define CUDA_TRY(expr)                                                                   \
+    do {                                                                                 \
+        cudaError_t e_ = (expr);                                                         \
+        if (e_ != cudaSuccess)                                                           \
+            return fail(FOMO_ECUDA, "%s failed: %s", #expr, cudaGetErrorString(e_));    \
+    } while (0)
+
+struct Object {
+    virtual ~Object() = default;
+};
+
+struct Buffer : Object {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+    ~Buffer() override {
+        if (ptr) cudaFree(ptr);
+    }
+};
+
+// Row pitch in floats: rows start on 128-byte boundaries.
+inline int pitch_of(int nx) { return (nx + 31) / 32 * 32; }
+
+struct Medium : Object {
+    int nx = 0, nz = 0, pitch = 0, M = 0, pad = 0, fs = 0;
+    float dx = 0, dz = 0;
+    float* base = nullptr;  // 5 arrays of pitch*nz floats
+    const float* arr(int q) const { return base + (size_t)q * pitch * nz; }
+    ~Medium() override {
+        if (base) cudaFree(base);
+    }
+};
+
+struct Wavefield : Object {
+    int nx = 0, nz = 0, pitch = 0;
+    float* base = nullptr;  // 2 copies x 5 fields of pitch*nz floats
+    int cur = 0;            // copy holding the current state
+    float* field(int copy, int q) const { return base + ((size_t)copy * 5 + q) * pitch * nz; }
+    ~Wavefield() override {
+        if (base) cudaFree(base);
+    }
+};
+
+struct Shot : Object {
+    uint64_t medium = 0, wavefield = 0;
+    int nbc = 0;
+    float q[5] = {0, 0, 0, 0, 0};
+    float a[fomo::kMaxM] = {0};
+    int M = 0;
+    float dt = 0, dtx = 0, dtz = 0;
+    int nt = 0, src_i = 0, src_j = 0, n_rec = 0, rec_kind = 0;
+    std::vector<float> wavelet;     // host copy: one sample per step
+    float* d_tabs = nullptr;        // 3 x (nbc+2)
+    int* d_rec = nullptr;           // n_rec linear offsets
+    float* d_gather = nullptr;      // nt x n_rec
+    int k_done = 0, recorded = 0;
+    double device_ms = 0;
+    int64_t launches = 0, h2d = 0, d2h = 0;
+    ~Shot() override {
+        if (d_tabs) cudaFree(d_tabs);
+        if (d_rec) cudaFree(d_rec);
+        if (d_gather) cudaFree(d_gather);
+    }
+};
+
+struct Context {
+    std::mutex mu;
+    bool inited = false;
+    int device = -1;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    uint64_t next = 1;
+    std::unordered_map<uint64_t, std::unique_ptr<Object>> objs;
+};
+
+Context& ctx() {
+    static Context c;
+    return c;
+}
+
+template <class T>
+T* get(uint64_t h) {
+    auto& C = ctx();
+    auto it = C.objs.find(h);
+    if (it == C.objs.end()) return nullptr;
+    return dynamic_cast<T*>(it->second.get());
+}
+
+uint64_t put(std::unique_ptr<Object> o) {
+    auto& C = ctx();
+    const uint64_t h = C.next++;
+    C.objs.emplace(h, std::move(o));
+    return h;
+}
+
+int ensure_init() {
+    if (!ctx().inited) return fail(FOMO_ENOINIT, "fomo_b200_init has not been called");
+    return FOMO_OK;
+}
+
+int check_medium_args(int nx, int nz, int M, int pad) {
+    if (M < 1 || M > fomo::kMaxM) return fail(FOMO_EINVAL, "M=%d out of range 1..%d", M, fomo::kMaxM);
+    if (nx < 2 * pad + 1 || nz < 2 * pad + 1)
+        return fail(FOMO_EINVAL, "grid %dx%d smaller than 2*pad+1 (pad=%d)", nx, nz, pad);
+    if (pad < M) return fail(FOMO_EINVAL, "pad=%d < M=%d", pad, M);
+    return FOMO_OK;
+}
+
+// Launch shape of one half step.
+struct Launch {
+    int tiles_x, tiles_z, n_tile, n_band;
+    size_t band_smem_v, band_smem_s;
+};
+
+Launch launch_shape(int nx, int nz, int nbc) {
+    Launch L;
+    L.tiles_x = (nx + fomo::kTileX - 1) / fomo::kTileX;
+    L.tiles_z = (nz + fomo::kTileZ - 1) / fomo::kTileZ;
+    L.n_tile = L.tiles_x * L.tiles_z;
+    L.n_band = (nx + fomo::kBandW - 1) / fomo::kBandW;
+    L.band_smem_v = 4 * (size_t)2 * ((size_t)(nbc + 1) * (fomo::kBandW + 6) + 2 * (fomo::kBandW + 2));
+    L.band_smem_s = 4 * (size_t)3 * ((size_t)(nbc + 1) * (fomo::kBandW + 6) + 2 * (fomo::kBandW + 2));
+    return L;
+}
+
+void fill_common(fomo::StepParams& P, const Medium& m, const Shot& s, const Launch& L) {
+    std::memset(&P, 0, sizeof(P));
+    P.nx = m.nx;
+    P.nz = m.nz;
+    P.pitch = m.pitch;
+    P.M = m.M;
+    P.pad = m.pad;
+    P.nbc = s.nbc;
+    P.fs = m.fs;
+    P.dtx = s.dtx;
+    P.dtz = s.dtz;
+    for (int l = 0; l < fomo::kMaxM; ++l) P.a[l] = s.a[l];
+    P.qx = s.q[0];
+    P.qz = s.q[1];
+    P.qt_x = s.q[2];
+    P.qt_z = s.q[3];
+    P.qxt = s.q[4];
+    for (int t = 0; t < 3; ++t) P.w_tab[t] = s.d_tabs + (size_t)t * (s.nbc + 2);
+    P.rho_vx = m.arr(0);
+    P.rho_vz = m.arr(1);
+    P.lam = m.arr(2);
+    P.mu_txx = m.arr(3);
+    P.mu_txz = m.arr(4);
+    P.src_i = s.src_i;
+    P.src_j = s.src_j;
+    P.nt = s.nt;
+    P.n_rec = s.n_rec;
+    P.rec_kind = s.rec_kind;
+    P.rec_cell = s.d_rec;
+    P.gather = s.d_gather;
+    P.tiles_x = L.tiles_x;
+    P.tiles_z = L.tiles_z;
+    P.n_tile_blocks = L.n_tile;
+    P.n_band_blocks = L.n_band;
+}
+
+// Per-launch event pairs, filled only by fomo_b200_shot_profile.
+struct Profile {
+    std::vector<cudaEvent_t> ev;      // 2 per launch
+    std::vector<int> kind;            // 0 velocity, 1 stress
+    int add(cudaStream_t st, int k) {
+        cudaEvent_t a, b;
+        if (cudaEventCreate(&a) != cudaSuccess || cudaEventCreate(&b) != cudaSuccess) return -1;
+        ev.push_back(a);
+        ev.push_back(b);
+        kind.push_back(k);
+        return cudaEventRecord(a, st) == cudaSuccess ? 0 : -1;
+    }
+    int end(cudaStream_t st) { return cudaEventRecord(ev.back(), st) == cudaSuccess ? 0 : -1; }
+    ~Profile() {
+        for (auto e : ev) cudaEventDestroy(e);
+    }
+};
+
+int run_steps(Shot& s, int n_steps, Profile* prof = nullptr) {
+    auto& C = ctx();
+    Medium* m = get<Medium>(s.medium);
+    Wavefield* w = get<Wavefield>(s.wavefield);
+    if (!m || !w) return fail(FOMO_EINVAL, "shot refers to a destroyed medium or wavefield");
+    const Launch L = launch_shape(m->nx, m->nz, s.nbc);
+    static size_t smem_set_v = 0, smem_set_s = 0;
+    if (L.band_smem_v > 48 * 1024 && L.band_smem_v > smem_set_v) {
+        CUDA_TRY(cudaFuncSetAttribute(fomo::velocity_simple_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)L.band_smem_v));
+        smem_set_v = L.band_smem_v;
+    }
+    if (L.band_smem_s > 48 * 1024 && L.band_smem_s > smem_set_s) {
+        CUDA_TRY(cudaFuncSetAttribute(fomo::stress_simple_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)L.band_smem_s));
+        smem_set_s = L.band_smem_s;
+    }
+    const int rec_blocks = (s.n_rec + 255) / 256;
+    CUDA_TRY(cudaEventRecord(C.ev0, C.stream));
+    const int k_end = std::min(s.nt, s.k_done + n_steps);
+    for (int k = s.k_done + 1; k <= k_end; ++k) {
+        const int a = w->cur, b = 1 - w->cur;
+        fomo::StepParams P;
+        fill_common(P, *m, s, L);
+        P.src_w = (k <= (int)s.wavelet.size()) ? s.wavelet[k - 1] : 0.f;
+        // velocity: reads v(a), tau(a); writes v(b); records step k-1 from copy a
+        for (int q = 0; q < 5; ++q) P.in[q] = w->field(a, q);
+        P.out[fomo::VX] = w->field(b, fomo::VX);
+        P.out[fomo::VZ] = w->field(b, fomo::VZ);
+        P.rec_k = (k >= 2 && s.n_rec > 0) ? k - 1 : 0;
+        const int vblocks = L.n_tile + L.n_band + (P.rec_k ? rec_blocks : 0);
+        if (prof && prof->add(C.stream, 0)) return fail(FOMO_ECUDA, "profiling event failed");
+        fomo::velocity_simple_kernel<<<vblocks, 256, L.band_smem_v, C.stream>>>(P);
+        if (prof && prof->end(C.stream)) return fail(FOMO_ECUDA, "profiling event failed");
+        // stress: reads v(b) (new), tau(a); writes tau(b)
+        P.in[fomo::VX] = w->field(b, fomo::VX);
+        P.in[fomo::VZ] = w->field(b, fomo::VZ);
+        for (int q = 2; q < 5; ++q) P.out[q] = w->field(b, q);
+        P.out[fomo::VX] = P.out[fomo::VZ] = nullptr;
+        P.rec_k = 0;
+        if (prof && prof->add(C.stream, 1)) return fail(FOMO_ECUDA, "profiling event failed");
+        fomo::stress_simple_kernel<<<L.n_tile + L.n_band, 256, L.band_smem_s, C.stream>>>(P);
+        if (prof && prof->end(C.stream)) return fail(FOMO_ECUDA, "profiling event failed");
+        s.launches += 2;
+        w->cur = b;
+        if (k >= 2) s.recorded = k - 1;
+        s.k_done = k;
+    }
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaEventRecord(C.ev1, C.stream));
+    CUDA_TRY(cudaEventSynchronize(C.ev1));
+    float ms = 0;
+    CUDA_TRY(cudaEventElapsedTime(&ms, C.ev0, C.ev1));
+    s.device_ms += ms;
+    return FOMO_OK;
+}
+
+// Records the receivers of the last step done (the next velocity launch would).
+int record_last(Shot& s) {
+    auto& C = ctx();
+    if (s.n_rec == 0 || s.k_done < 1 || s.recorded >= s.k_done) return FOMO_OK;
+    Medium* m = get<Medium>(s.medium);
+    Wavefield* w = get<Wavefield>(s.wavefield);
+    if (!m || !w) return fail(FOMO_EINVAL, "shot refers to a destroyed medium or wavefield");
+    const Launch L = launch_shape(m->nx, m->nz, s.nbc);
+    fomo::StepParams P;
+    fill_common(P, *m, s, L);
+    for (int q = 0; q < 5; ++q) P.in[q] = w->field(w->cur, q);
+    P.rec_k = s.k_done;
+    fomo::record_kernel<<<(s.n_rec + 255) / 256, 256, 0, C.stream>>>(P);
+    CUDA_TRY(cudaGetLastError());
+    s.launches += 1;
+    s.recorded = s.k_done;
+    return FOMO_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int fomo_b200_version(void) { return 100; }
+
+const char* fomo_b200_last_error(void) { return g_err.c_str(); }
+
+int fomo_b200_init(int device) {
+    auto& C = ctx();
+    std::lock_guard<std::mutex> lk(C.mu);
+    if (C.inited) {
+        if (C.device == device) return FOMO_OK;
+        return fail(FOMO_EINVAL, "already initialised on device %d", C.device);
+    }
+    int n = 0;
+    CUDA_TRY(cudaGetDeviceCount(&n));
+    if (device < 0 || device >= n) return fail(FOMO_EINVAL, "device %d not present (%d devices)", device, n);
+    CUDA_TRY(cudaSetDevice(device));
+    cudaDeviceProp prop;
+    CUDA_TRY(cudaGetDeviceProperties(&prop, device));
+    if (prop.major != 10) return fail(FOMO_ECUDA, "device %d is sm_%d%d; this library is built for sm_100a", device, prop.major, prop.minor);
+    CUDA_TRY(cudaStreamCreateWithFlags(&C.stream, cudaStreamNonBlocking));
+    CUDA_TRY(cudaEventCreate(&C.ev0));
+    CUDA_TRY(cudaEventCreate(&C.ev1));
+    C.device = device;
+    C.inited = true;
+    return FOMO_OK;
+}
+
+int fomo_b200_shutdown(void) {
+    auto& C = ctx();
+    std::lock_guard<std::mutex> lk(C.mu);
+    if (!C.inited) return FOMO_OK;
+    cudaStreamSynchronize(C.stream);
+    C.objs.clear();
+    cudaEventDestroy(C.ev0);
+    cudaEventDestroy(C.ev1);
+    cudaStreamDestroy(C.stream);
+    C.stream = nullptr;
+    C.inited = false;
+    C.device = -1;
+    return FOMO_OK;
+}
+
+int fomo_b200_synchronize(void) {
+    std::lock_guard<std::mutex> lk(ctx().mu);
+    if (int rc = ensure_init()) return rc;
+    CUDA_TRY(cudaStreamSynchronize(ctx().stream));
+    return FOMO_OK;
+}
+
+int fomo_b200_get_stream(void** stream) {
+    std::lock_guard<std::mutex> lk(ctx().mu);
+    if (int rc = ensure_init()) return rc;
+    if (!stream) return fail(FOMO_EINVAL, "stream is NULL");
+    *stream = (void*)ctx().stream;
+    return FOMO_OK;
+}
+
+// ---------------------------------------------------------------- buffers
+int fomo_b200_alloc(size_t bytes, uint64_t* handle) {
+    std::lock_guard<std::mutex> lk(ctx().mu);
+    if (int rc = ensure_init()) return rc;
+    if (!handle) return fail(FOMO_EINVAL, "handle is NULL");
+    auto b = std::make_unique<Buffer>();
+    if (bytes) {
+        cudaError_t e = cudaMalloc(&b->ptr, bytes);
+        if (e != cudaSuccess) return fail(FOMO_ENOMEM, "cudaMalloc(%zu) failed: %s", bytes, cudaGetErrorString(e));
+    }
+    b->bytes = bytes;
+    *handle = put(std::move(b));
+    return FOMO_OK;
+}
+
+int fomo_b200_upload(uint64_t handle, const void* host, size_t bytes) {
+    std::lock_guard<std::mutex> lk(ctx().mu);
+    if (int rc = ensure_init()) return rc;
+    Buffer* b = get<Buffer>(handle);
+    if (!b) return fail(FOMO_EINVAL, "unknown buffer handle %llu", (unsigned long long)handle);
+    if (bytes > b->bytes || (bytes && !host)) return fail(FOMO_EINVAL, "upload of %zu bytes into a %zu-byte buffer", bytes, b->bytes);
+    CUDA_TRY(cudaMemcpyAsync(b->ptr, host, bytes, cudaMemcpyHostToDevice, ctx().stream));
+    CUDA_TRY(cudaStreamSynchronize(ctx().stream));
+    return FOMO_OK;
+}
+
+int fomo_b200_download(uint64_t handle, void* host, size_t bytes) {
+    std::lock_guard<std::mutex> lk(ctx().mu);
+    if (int rc = ensure_init()) return rc;
+    Buffer* b = get<Buffer>(handle);
+    if (!b) return fail(FOMO_EINVAL, "unknown buffer handle %llu", (unsigned long long)handle);
+    if (bytes > b->bytes || (bytes && !host)) return fail(FOMO_EINVAL, "download of %zu bytes from a %zu-byte buffer", bytes, b->bytes);
+    CUDA_TRY(cudaMemcpyAsync(host, b->ptr, bytes, cudaMemcpyDeviceToHost, ctx().stream));
+    CUDA_TRY(cudaStreamSynchronize(ctx().stream));
+    return FOMO_OK;
+}
+
+int fomo_b200_memset(uint64_t handle, float value) {
+    std::lock_guard<std::mutex> lk(ctx().mu);
+    if (int rc = ensure_init()) return rc;
+    Buffer* b = get<Buffer>(handle);
+    if (!b) return fail(FOMO_EINVAL, "unknown buffer handle %llu", (unsigned long long)handle);
+    if (b->bytes % 4) return fail(FOMO_EINVAL, "buffer of %zu bytes is not a Float32 array", b->bytes);
+    if (value == 0.f) {
+        CUDA_TRY(cudaMemsetAsync(b->ptr, 0, b->bytes, ctx().stream));
+    } else {
+        std::vector<float> h(b->bytes / 4, value);
+        CUDA_TRY(cudaMemcpyAsync(b->ptr, h.data(), b->bytes, cudaMemcpyHostToDevice, ctx().stream));
+    }
+    CUDA_TRY(cudaStreamSynchronize(ctx().stream));
+    return FOMO_OK;
+}
+
+int fomo_b200_free(uint64_t handle) {
+    std::lock_guard<std::mutex> lk(ctx().mu);
+    if (int rc = ensure_init()) return rc;
+    if (!get<Buffer>(handle)) return fail(FOMO_EINVAL, "unknown buffer handle %llu", (unsigned long long)handle);
+    cudaStreamSynchronize(ctx().stream);
+    ctx().objs.erase(handle);
+    return FOMO_OK;
+}
+
+// ---------------------------------------------------------------- medium
+int fomo_b200_medium_create(int32_t nx, int32_t nz, int32_t M, int32_t pad, int32_t free_surface,
+                            float dx, float dz, const float* rho_vx, const float* rho_vz, const float* lam,
+                            const float* mu_txx, const float* mu_txz, uint64_t* medium) {
+    std::lock_guard<std::mutex> lk(ctx().mu);
+    if (int rc = ensure_init()) return rc;
+    if (!medium || !rho_vx || !rho_vz || !lam || !mu_txx || !mu_txz) return fail(FOMO_EINVAL, "NULL pointer argument");
+    if (int rc = check_medium_args(nx, nz, M, pad)) return rc;
+    if (free_surface && pad < 5) return fail(FOMO_EINVAL, "free surface needs pad >= 5 (rows pad-4..pad+1), got %d", pad);
+    auto m = std::make_unique<Medium>();
+    m->nx = nx;
+    m->nz = nz;
+    m->pitch = pitch_of(nx);
+    m->M = M;
+    m->pad = pad;
+    m->fs = free_surface ? 1 : 0;
+    m->dx = dx;
+    m->dz = dz;
+    const size_t plane = (size_t)m->pitch * nz;
+    cudaError_t e = cudaMalloc(&m->base, 5 * plane * sizeof(float));
+    if (e != cudaSuccess) return fail(FOMO_ENOMEM, "medium allocation failed: %s", cudaGetErrorString(e));
+    const float* src[5] = {rho_vx, rho_vz, lam, mu_txx, mu_txz};
+    for (int q = 0; q < 5; ++q)
+        CUDA_TRY(cudaMemcpy2DAsync(m->base + q * plane, m->pitch * sizeof(float), src[q], nx * sizeof(float),
+                                   nx * sizeof(float), nz, cudaMemcpyHostToDevice, ctx().stream));
+    CUDA_TRY(cudaStreamSynchronize(ctx().stream));
+    *medium = put(std::move(m));
+    return FOMO_OK;
+}
+
+int fomo_b200_medium_destroy(uint64_t medium) {
+    std::lock_guard<std::mutex> lk(ctx().mu);
+    if (int rc = ensure_init()) return rc;
+    if (!get<Medium>(medium)) return fail(FOMO_EINVAL, "unknown medium handle %llu", (unsigned long long)medium);
+    cudaStreamSynchronize(ctx().stream);
+    ctx().objs.erase(medium);
+    return FOMO_OK;
+}
+
+// ---------------------------------------------------------------- wavefield
+int fomo_b200_wavefield_create(int32_t nx, int32_t nz, uint64_t* wavefield) {
+    std::lock_guard<std::mutex> lk(ctx().mu);
+    if (int rc = ensure_init()) return rc;
+    if (!wavefield || nx < 3 || nz < 3) return fail(FOMO_EINVAL, "bad wavefield size %dx%d", nx, nz);
+    auto w = std::make_unique<Wavefield>();
+    w->nx = nx;
+    w->nz = nz;
+    w->pitch = pitch_of(nx);
+    const size_t bytes = 10 * (size_t)w->pitch * nz * sizeof(float);
+    cudaError_t e = cudaMalloc(&w->base, bytes);
+    if (e != cudaSuccess) return fail(FOMO_ENOMEM, "wavefield allocation of %zu bytes failed: %s", bytes, cudaGetErrorString(e));
+    CUDA_TRY(cudaMemsetAsync(w->base, 0, bytes, ctx().stream));
+    CUDA_TRY(cudaStreamSynchronize(ctx().stream));
+    *wavefield = put(std::move(w));
+    return FOMO_OK;
+}
+
+int fomo_b200_wavefield_destroy(uint64_t wavefield) {
+    std::lock_guard<std::mutex> lk(ctx().mu);
+    if (int rc = ensure_init()) return rc;
+    if (!get<Wavefield>(wavefield)) return fail(FOMO_EINVAL, "unknown wavefield handle %llu", (unsigned long long)wavefield);
+    cudaStreamSynchronize(ctx().stream);
+    ctx().objs.erase(wavefield);
+    return FOMO_OK;
+}
+
+static int wavefield_reset_locked(Wavefield* w) {
+    CUDA_TRY(cudaMemsetAsync(w->base, 0, 10 * (size_t)w->pitch * w->nz * sizeof(float), ctx().stream));
+    w->cur = 0;
+    return FOMO_OK;
+}
+
+int fomo_b200_wavefield_reset(uint64_t wavefield) {
+    std::lock_guard<std::mutex> lk(ctx().mu);
+    if (int rc = ensure_init()) return rc;
+    Wavefield* w = get<Wavefield>(wavefield);
+    if (!w) return fail(FOMO_EINVAL, "unknown wavefield handle %llu", (unsigned long long)wavefield);
+    if (int rc = wavefield_reset_locked(w)) return rc;
+    CUDA_TRY(cudaStreamSynchronize(ctx().stream));
+    return FOMO_OK;
+}
+
+int fomo_b200_wavefield_download(uint64_t wavefield, int32_t field, float* host) {
+    std::lock_guard<std::mutex> lk(ctx().mu);
+    if (int rc = ensure_init()) return rc;
+    Wavefield* w = get<Wavefield>(wavefield);
+    if (!w) return fail(FOMO_EINVAL, "unknown wavefield handle %llu", (unsigned long long)wavefield);
+    if (field < 0 || field > 4 || !host) return fail(FOMO_EINVAL, "bad field %d or NULL host pointer", field);
+    CUDA_TRY(cudaMemcpy2DAsync(host, w->nx * sizeof(float), w->field(w->cur, field), w->pitch * sizeof(float),
+                               w->nx * sizeof(float), w->nz, cudaMemcpyDeviceToHost, ctx().stream));
+    CUDA_TRY(cudaStreamSynchronize(ctx().stream));
+    return FOMO_OK;
+}
+
+int fomo_b200_wavefield_upload(uint64_t wavefield, int32_t field, const float* host) {
+    std::lock_guard<std::mutex> lk(ctx().mu);
+    if (int rc = ensure_init()) return rc;
+    Wavefield* w = get<Wavefield>(wavefield);
+    if (!w) return fail(FOMO_EINVAL, "unknown wavefield handle %llu", (unsigned long long)wavefield);
+    if (field < 0 || field > 4 || !host) return fail(FOMO_EINVAL, "bad field %d or NULL host pointer", field);
+    CUDA_TRY(cudaMemcpy2DAsync(w->field(w->cur, field), w->pitch * sizeof(float), host, w->nx * sizeof(float),
+                               w->nx * sizeof(float), w->nz, cudaMemcpyHostToDevice, ctx().stream));
+    CUDA_TRY(cudaStreamSynchronize(ctx().stream));
+    return FOMO_OK;
+}
+
+// ---------------------------------------------------------------- shots
+int fomo_b200_shot_begin(uint64_t medium, uint64_t wavefield, const FomoHabc* habc, const FomoShot* shot,
+                         uint64_t* shot_handle) {
+    std::lock_guard<std::mutex> lk(ctx().mu);
+    if (int rc = ensure_init()) return rc;
+    Medium* m = get<Medium>(medium);
+    Wavefield* w = get<Wavefield>(wavefield);
+    if (!m) return fail(FOMO_EINVAL, "unknown medium handle %llu", (unsigned long long)medium);
+    if (!w) return fail(FOMO_EINVAL, "unknown wavefield handle %llu", (unsigned long long)wavefield);
+    if (!habc || !shot || !shot_handle) return fail(FOMO_EINVAL, "NULL argument");
+    if (w->nx != m->nx || w->nz != m->nz)
+        return fail(FOMO_EINVAL, "wavefield %dx%d does not match medium %dx%d", w->nx, w->nz, m->nx, m->nz);
+    if (shot->M != m->M) return fail(FOMO_EINVAL, "shot M=%d differs from medium M=%d", shot->M, m->M);
+    if (!shot->a) return fail(FOMO_EINVAL, "FD coefficients are NULL");
+    if (shot->nt < 0) return fail(FOMO_EINVAL, "nt=%d < 0", shot->nt);
+    const int nbc = habc->nbc;
+    if (nbc < 1 || 2 * nbc + 3 > m->nx || 2 * nbc + 2 > m->nz)
+        return fail(FOMO_EINVAL, "nbc=%d does not fit the %dx%d grid", nbc, m->nx, m->nz);
+    if (!habc->w_vx || !habc->w_vz || !habc->w_tau) return fail(FOMO_EINVAL, "HABC weight tables are NULL");
+    if (shot->src_i < 1 || shot->src_i > m->nx || shot->src_j < 1 || shot->src_j > m->nz)
+        return fail(FOMO_EINVAL, "source (%d, %d) outside the %dx%d grid", shot->src_i, shot->src_j, m->nx, m->nz);
+    if (shot->n_wavelet < 0 || (shot->n_wavelet > 0 && !shot->wavelet)) return fail(FOMO_EINVAL, "bad wavelet");
+    if (shot->n_rec < 0 || (shot->n_rec > 0 && (!shot->rec_i || !shot->rec_j)))
+        return fail(FOMO_EINVAL, "bad receiver arrays");
+    if (shot->rec_kind < 0 || shot->rec_kind > 2) return fail(FOMO_EINVAL, "bad receiver kind %d", shot->rec_kind);
+    std::vector<int> cells(shot->n_rec);
+    for (int r = 0; r < shot->n_rec; ++r) {
+        const int i = shot->rec_i[r], j = shot->rec_j[r];
+        if (i < 1 || i > m->nx || j < 1 || j > m->nz)
+            return fail(FOMO_EINVAL, "receiver %d at (%d, %d) outside the %dx%d grid", r + 1, i, j, m->nx, m->nz);
+        cells[r] = (i - 1) + (j - 1) * m->pitch;
+    }
+    auto s = std::make_unique<Shot>();
+    s->medium = medium;
+    s->wavefield = wavefield;
+    s->nbc = nbc;
+    s->q[0] = habc->qx;
+    s->q[1] = habc->qz;
+    s->q[2] = habc->qt_x;
+    s->q[3] = habc->qt_z;
+    s->q[4] = habc->qxt;
+    s->M = shot->M;
+    for (int l = 0; l < shot->M; ++l) s->a[l] = shot->a[l];
+    s->dt = shot->dt;
+    s->dtx = shot->dtx;
+    s->dtz = shot->dtz;
+    s->nt = shot->nt;
+    s->src_i = shot->src_i - 1;
+    s->src_j = shot->src_j - 1;
+    s->wavelet.assign(shot->wavelet, shot->wavelet + shot->n_wavelet);
+    s->n_rec = shot->n_rec;
+    s->rec_kind = shot->rec_kind;
+    const size_t tab_n = (size_t)nbc + 2;
+    cudaError_t e = cudaMalloc(&s->d_tabs, 3 * tab_n * sizeof(float));
+    if (e == cudaSuccess && s->n_rec) e = cudaMalloc(&s->d_rec, s->n_rec * sizeof(int));
+    if (e == cudaSuccess && s->n_rec && s->nt)
+        e = cudaMalloc(&s->d_gather, (size_t)s->nt * s->n_rec * sizeof(float));
+    if (e != cudaSuccess) return fail(FOMO_ENOMEM, "shot allocation failed: %s", cudaGetErrorString(e));
+    cudaStream_t st = ctx().stream;
+    CUDA_TRY(cudaMemcpyAsync(s->d_tabs, habc->w_vx, tab_n * 4, cudaMemcpyHostToDevice, st));
+    CUDA_TRY(cudaMemcpyAsync(s->d_tabs + tab_n, habc->w_vz, tab_n * 4, cudaMemcpyHostToDevice, st));
+    CUDA_TRY(cudaMemcpyAsync(s->d_tabs + 2 * tab_n, habc->w_tau, tab_n * 4, cudaMemcpyHostToDevice, st));
+    s->h2d += 3 * tab_n * 4;
+    if (s->n_rec) {
+        CUDA_TRY(cudaMemcpyAsync(s->d_rec, cells.data(), s->n_rec * sizeof(int), cudaMemcpyHostToDevice, st));
+        s->h2d += s->n_rec * 8;
+        if (s->nt) CUDA_TRY(cudaMemsetAsync(s->d_gather, 0, (size_t)s->nt * s->n_rec * sizeof(float), st));
+    }
+    s->h2d += (int64_t)s->wavelet.size() * 4;
+    if (int rc = wavefield_reset_locked(w)) return rc;
+    CUDA_TRY(cudaStreamSynchronize(st));
+    *shot_handle = put(std::move(s));
+    return FOMO_OK;
+}
+
+int fomo_b200_shot_advance(uint64_t shot_handle, int32_t n_steps, int32_t* k_done) {
+    std::lock_guard<std::mutex> lk(ctx().mu);
+    if (int rc = ensure_init()) return rc;
+    Shot* s = get<Shot>(shot_handle);
+    if (!s) return fail(FOMO_EINVAL, "unknown shot handle %llu", (unsigned long long)shot_handle);
+    if (n_steps < 0) return fail(FOMO_EINVAL, "n_steps=%d < 0", n_steps);
+    if (int rc = run_steps(*s, n_steps)) return rc;
+    if (k_done) *k_done = s->k_done;
+    return FOMO_OK;
+}
+
+int fomo_b200_shot_finish(uint64_t shot_handle, float* gather_out, FomoRunStats* stats) {
+    std::lock_guard<std::mutex> lk(ctx().mu);
+    if (int rc = ensure_init()) return rc;
+    Shot* s = get<Shot>(shot_handle);
+    if (!s) return fail(FOMO_EINVAL, "unknown shot handle %llu", (unsigned long long)shot_handle);
+    if (int rc = record_last(*s)) return rc;
+    if (gather_out && s->n_rec && s->nt) {
+        const size_t bytes = (size_t)s->nt * s->n_rec * sizeof(float);
+        CUDA_TRY(cudaMemcpyAsync(gather_out, s->d_gather, bytes, cudaMemcpyDeviceToHost, ctx().stream));
+        s->d2h += bytes;
+    }
+    CUDA_TRY(cudaStreamSynchronize(ctx().stream));
+    if (stats) {
+        stats->device_ms = s->device_ms;
+        stats->steps = s->k_done;
+        stats->kernel_launches = s->launches;
+        stats->h2d_bytes = s->h2d;
+        stats->d2h_bytes = s->d2h;
+    }
+    ctx().objs.erase(shot_handle);
+    return FOMO_OK;
+}
+
+int fomo_b200_shot_profile(uint64_t shot_handle, int32_t n_steps, FomoKernelTime* out, int32_t max_kinds,
+                           int32_t* n_kinds) {
+    std::lock_guard<std::mutex> lk(ctx().mu);
+    if (int rc = ensure_init()) return rc;
+    Shot* s = get<Shot>(shot_handle);
+    if (!s) return fail(FOMO_EINVAL, "unknown shot handle %llu", (unsigned long long)shot_handle);
+    if (n_steps < 0 || n_steps > 100000 || !out || !n_kinds || max_kinds < 2)
+        return fail(FOMO_EINVAL, "bad profile arguments");
+    Medium* m = get<Medium>(s->medium);
+    if (!m) return fail(FOMO_EINVAL, "shot refers to a destroyed medium");
+    Profile prof;
+    if (int rc = run_steps(*s, n_steps, &prof)) return rc;
+    CUDA_TRY(cudaStreamSynchronize(ctx().stream));
+    // Algorithmic bytes of one launch over the nx*nz cells: velocity reads
+    // vx, vz, txx, tzz, txz, rho_vx, rho_vz and writes vx, vz (36 B/cell);
+    // stress reads vx, vz, txx, tzz, txz, lam, mu_txx, mu_txz and writes
+    // txx, tzz, txz (44 B/cell).
+    const double cells = (double)m->nx * m->nz;
+    const char* names[2] = {"velocity", "stress"};
+    const double bpc[2] = {36.0, 44.0};
+    for (int k = 0; k < 2; ++k) {
+        std::memset(&out[k], 0, sizeof(FomoKernelTime));
+        std::snprintf(out[k].name, sizeof(out[k].name), "%s", names[k]);
+        out[k].bytes_per_launch = bpc[k] * cells;
+    }
+    for (size_t i = 0; i < prof.kind.size(); ++i) {
+        float ms = 0;
+        CUDA_TRY(cudaEventElapsedTime(&ms, prof.ev[2 * i], prof.ev[2 * i + 1]));
+        out[prof.kind[i]].launches += 1;
+        out[prof.kind[i]].total_ms += ms;
+    }
+    *n_kinds = 2;
+    return FOMO_OK;
+}
+
+int fomo_b200_run_shot(uint64_t medium, uint64_t wavefield, const FomoHabc* habc, const FomoShot* shot,
+                       float* gather_out, FomoRunStats* stats) {
+    uint64_t h = 0;
+    if (int rc = fomo_b200_shot_begin(medium, wavefield, habc, shot, &h)) return rc;
+    int32_t k = 0;
+    if (int rc = fomo_b200_shot_advance(h, shot->nt, &k)) {
+        std::string msg = g_err;
+        fomo_b200_shot_finish(h, nullptr, nullptr);
+        g_err = msg;
+        return rc;
+    }
+    return fomo_b200_shot_finish(h, gather_out, stats);
+}
+
+}  // extern "C"

@@ -1,0 +1,208 @@
+/*
+ * fomo_b200.h -- C ABI of libfomo_b200.so, the B200 (sm_100a) engine for the
+ * time-stepping path of Wuheng10086/Fomo_julia's Elastic2D module.
+ *
+ * This is the boundary a `backend(:b200)` for the reference binds through
+ * `ccall`: plain pointers, sizes and opaque 64-bit handles, no C++ or torch
+ * types.  Each declaration names the reference interface it stands in for
+ * (paths inside Wuheng10086/Fomo_julia).
+ *
+ * Conventions
+ *   - Every function returns an int status: FOMO_OK (0) or a negative
+ *     FOMO_E* code; fomo_b200_last_error() then holds a message for the
+ *     calling thread.
+ *   - Grids are the reference's padded (nx, nz) Float32 matrices, column
+ *     major with x fastest: element (i, j) (1-based) at (i-1) + (j-1)*nx.
+ *   - Grid indices passed in (source, receivers) are 1-based, as Julia
+ *     passes them.
+ *   - Host pointers are borrowed for the duration of the call only.  The
+ *     library owns all device memory it allocates.
+ *   - Gathers are [nt x n_rec] column major: sample k (1-based) of receiver r
+ *     (1-based) at (k-1) + (r-1)*nt, exactly the reference's Receivers.data.
+ */
+#ifndef FOMO_B200_H
+#define FOMO_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FOMO_OK          0
+#define FOMO_EINVAL     -1   /* invalid argument, size or handle            */
+#define FOMO_ENOMEM     -2   /* device allocation failed / over HBM budget  */
+#define FOMO_ECUDA      -3   /* a CUDA runtime or driver call failed        */
+#define FOMO_ETIMEOUT   -4   /* a bounded device-side wait gave up          */
+#define FOMO_ECANCELLED -5   /* a queued request was cancelled              */
+#define FOMO_ENOTREADY  -6   /* request not finished yet (poll)             */
+#define FOMO_ENOINIT    -7   /* fomo_b200_init has not been called          */
+
+/* Receiver components: Receivers.type (src/core/Structures.jl:127-132). */
+#define FOMO_REC_VZ 0
+#define FOMO_REC_VX 1
+#define FOMO_REC_P  2        /* (txx + tzz) * 0.5, as the CPU method does   */
+
+/* Wavefield components, in the order of Wavefield's fields. */
+#define FOMO_FIELD_VX  0
+#define FOMO_FIELD_VZ  1
+#define FOMO_FIELD_TXX 2
+#define FOMO_FIELD_TZZ 3
+#define FOMO_FIELD_TXZ 4
+
+/* ---------------------------------------------------------------------- */
+/* Library lifetime                                                        */
+/* ---------------------------------------------------------------------- */
+
+/* Selects the CUDA device and creates the library's stream.  Stands in for
+ * the CUDA probe of src/Elastic2D.jl:24-34 and backend(:cuda) in
+ * src/backends/backend.jl:39-53. */
+int fomo_b200_init(int device);
+
+/* Frees every handle and the stream. */
+int fomo_b200_shutdown(void);
+
+/* Message for the last failing call on this thread ("" if none); stands in
+ * for the reference's error(...) strings (src/backends/backend.jl:49). */
+const char* fomo_b200_last_error(void);
+
+/* Version as major*10000 + minor*100 + patch. */
+int fomo_b200_version(void);
+
+/* ---------------------------------------------------------------------- */
+/* Raw device buffers (backing store of a B200Matrix / B200Vector)         */
+/* ---------------------------------------------------------------------- */
+
+/* to_device(data, backend) (src/backends/backend.jl:68-71) = alloc + upload;
+ * Array(x) = download; fill!(x, v) = memset. */
+int fomo_b200_alloc(size_t bytes, uint64_t* handle);
+int fomo_b200_upload(uint64_t handle, const void* host, size_t bytes);
+int fomo_b200_download(uint64_t handle, void* host, size_t bytes);
+int fomo_b200_memset(uint64_t handle, float value);
+int fomo_b200_free(uint64_t handle);
+
+/* synchronize(::CUDABackend) (src/backends/backend.jl:78-79). */
+int fomo_b200_synchronize(void);
+
+/* The library's CUDA stream (a cudaStream_t), so a caller can order its own
+ * work or timing events against the library's kernels.  No reference
+ * counterpart: CUDA.jl's task-local stream plays this role there. */
+int fomo_b200_get_stream(void** stream);
+
+/* ---------------------------------------------------------------------- */
+/* Medium: Medium{T} (src/core/Structures.jl:66-83) as built by           */
+/* init_medium (src/utils/init.jl:68-99).                                  */
+/* ---------------------------------------------------------------------- */
+
+/* Uploads the five staggered material arrays of a padded (nx, nz) grid.
+ * M = fd_order/2 (1..6), pad = nbc + M, free_surface 0/1. */
+int fomo_b200_medium_create(int32_t nx, int32_t nz, int32_t M, int32_t pad,
+                            int32_t free_surface, float dx, float dz,
+                            const float* rho_vx, const float* rho_vz,
+                            const float* lam, const float* mu_txx,
+                            const float* mu_txz, uint64_t* medium);
+int fomo_b200_medium_destroy(uint64_t medium);
+
+/* ---------------------------------------------------------------------- */
+/* HABC: HABCConfig{T} (src/core/Structures.jl:94-105) as built by         */
+/* init_habc (src/utils/init.jl:171-203).                                  */
+/* ---------------------------------------------------------------------- */
+
+/* The reference stores each weight as a full (nz, nx) matrix, but every
+ * entry is a function of dist = min(i-1, nx-i, j-1, nz-j) alone
+ * (init.jl:188-195); the three tables give that function for
+ * dist = 0..nbc+1 (larger distances use entry nbc+1). */
+typedef struct {
+    int32_t nbc;
+    float qx, qz, qt_x, qt_z, qxt;
+    const float* w_vx;    /* host, nbc+2 entries */
+    const float* w_vz;
+    const float* w_tau;
+} FomoHabc;
+
+/* ---------------------------------------------------------------------- */
+/* Wavefield{T} (src/core/Structures.jl:18-55)                             */
+/* ---------------------------------------------------------------------- */
+
+/* Wavefield(nx, nz, backend): device state of one shot.  The B200 engine
+ * keeps two copies of the five fields (the step reads one, writes the
+ * other); the reference's five *_old boundary strips are the copy being
+ * read, so no separate backup pass exists. */
+int fomo_b200_wavefield_create(int32_t nx, int32_t nz, uint64_t* wavefield);
+int fomo_b200_wavefield_destroy(uint64_t wavefield);
+/* reset!(backend, W) (src/kernels/source_receiver.jl:115-133). */
+int fomo_b200_wavefield_reset(uint64_t wavefield);
+/* Array(W.vx) etc.: copies the current value of one field (FOMO_FIELD_*)
+ * into host[nx*nz]. */
+int fomo_b200_wavefield_download(uint64_t wavefield, int32_t field, float* host);
+/* to_device into W.vx etc.: overwrites the current value of one field. */
+int fomo_b200_wavefield_upload(uint64_t wavefield, int32_t field, const float* host);
+
+/* ---------------------------------------------------------------------- */
+/* One shot: Source (Structures.jl:116-120), Receivers (:127-132),         */
+/* SimParams (:143-155) and the FD coefficients (init.jl:13-29).           */
+/* ---------------------------------------------------------------------- */
+
+typedef struct {
+    const float* a;        /* host, M FD coefficients                        */
+    int32_t M;             /* must equal the medium's M                      */
+    float dt, dtx, dtz;    /* SimParams: dtx = Float32(dt/dx) etc.           */
+    int32_t nt;            /* time steps                                     */
+    int32_t src_i, src_j;  /* 1-based source cell (explosive: txx and tzz)   */
+    const float* wavelet;  /* host, n_wavelet samples; step k > n_wavelet    */
+    int32_t n_wavelet;     /*   injects nothing (source_receiver.jl:19-21)   */
+    int32_t n_rec;         /* receivers (0 allowed)                          */
+    const int32_t* rec_i;  /* host, 1-based                                  */
+    const int32_t* rec_j;
+    int32_t rec_kind;      /* FOMO_REC_*                                     */
+} FomoShot;
+
+typedef struct {
+    double device_ms;      /* device time of the time loop (CUDA events)     */
+    int64_t steps;         /* time steps run                                 */
+    int64_t kernel_launches;/* kernels launched by the library for the loop  */
+    int64_t h2d_bytes;     /* host->device bytes moved by the call           */
+    int64_t d2h_bytes;     /* device->host bytes moved by the call           */
+} FomoRunStats;
+
+/* run_shot! (src/simulation/shot_manager.jl:46-68) with run_time_loop!
+ * (src/simulation/time_stepper.jl:97-128) and time_step! (:39-63):
+ * resets the wavefield, runs nt steps and writes the gather to
+ * gather_out[nt*n_rec] (host).  The call blocks until the gather is on the
+ * host.  stats may be NULL. */
+int fomo_b200_run_shot(uint64_t medium, uint64_t wavefield, const FomoHabc* habc,
+                       const FomoShot* shot, float* gather_out, FomoRunStats* stats);
+
+/* The same loop in chunks, for an on_step callback (time_stepper.jl:112-119):
+ * begin resets the wavefield and uploads the shot; advance runs up to
+ * n_steps more steps (returns the number of steps done so far in *k_done);
+ * the wavefield can be downloaded between advances; finish copies the
+ * gather (the first k_done rows are valid) and releases the shot.  A shot
+ * stopped early is finished like a complete one. */
+int fomo_b200_shot_begin(uint64_t medium, uint64_t wavefield, const FomoHabc* habc,
+                         const FomoShot* shot, uint64_t* shot_handle);
+int fomo_b200_shot_advance(uint64_t shot_handle, int32_t n_steps, int32_t* k_done);
+int fomo_b200_shot_finish(uint64_t shot_handle, float* gather_out, FomoRunStats* stats);
+
+/* Per-kernel timing of a shot's loop (no reference counterpart; used by
+ * bench.py for the roofline).  Runs up to n_steps more steps of the shot
+ * with CUDA events around every launch and reports, per kernel kind, the
+ * launches, their summed device time and the algorithmic DRAM bytes of one
+ * launch (the bytes a launch must move at minimum: each array it reads
+ * once and each array it writes once, over the cells it updates). */
+typedef struct {
+    char name[32];
+    int64_t launches;
+    double total_ms;
+    double bytes_per_launch;
+} FomoKernelTime;
+
+int fomo_b200_shot_profile(uint64_t shot_handle, int32_t n_steps, FomoKernelTime* out,
+                           int32_t max_kinds, int32_t* n_kinds);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FOMO_B200_H */

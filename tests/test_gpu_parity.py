@@ -1,0 +1,142 @@
+"""GPU path (libfomo_b200.so through the C ABI) against the CPU oracle.
+
+The kernels evaluate the reference's Float32 expressions in the same order
+with IEEE rounding, so gathers and final wavefields are expected to be
+bit-identical to the oracle; the acceptance bar stated by the spec
+(relative L2 <= 1e-5 per trace) is asserted as well.
+"""
+import numpy as np
+import pytest
+
+import fomo_julia_b200 as F
+from cases import Case, golden_gather, layered, oracle_inputs, per_trace_rel_l2, runjl_case
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-5
+FIELDS = ("vx", "vz", "txx", "tzz", "txz")
+
+
+def gpu_run(c: Case, b200, on_step=None, step_chunk=1, W=None):
+    med = F.init_medium(c.vp, c.vs, c.rho, c.dx, c.dz, c.nbc, c.fd_order, b200, free_surface=c.free_surface)
+    H = F.init_habc(med.nx, med.nz, c.nbc, c.dt, c.dx, c.dz, c.v_ref, b200)
+    params = F.sim_params(c.dt, c.nt, c.dx, c.dz, c.fd_order)
+    a = F.get_fd_coefficients(c.fd_order)
+    wav = F.ricker_wavelet(c.f0, c.dt, c.nt)
+    rec = F.setup_receivers(c.rec_x, c.rec_z, med, type=c.rec_type)
+    src = F.Source(F.coord_to_index(c.src_x, med.dx, med.pad), F.coord_to_index(c.src_z, med.dz, med.pad), wav)
+    own_w = W is None
+    W = W or F.Wavefield(med.nx, med.nz, b200)
+    r = F.run_shot(b200, W, med, H, a, src, rec, params, on_step=on_step, step_chunk=step_chunk)
+    fields = {f: W.field(f) for f in FIELDS}
+    if own_w:
+        W.release()
+    med.release()
+    return r, fields
+
+
+def oracle_run(c: Case, oracle, n_steps=None):
+    med, h, a, wav, si, sj, ri, rj = oracle_inputs(c, oracle)
+    g, fin = oracle.run_shot(med, h, a, c.dt, c.nt, si, sj, wav, ri, rj, c.rec_type, "simd8",
+                             final_fields=True, n_steps=n_steps)
+    return g, {f: fin[:, :, q] for q, f in enumerate(FIELDS)}
+
+
+def assert_same(g_gpu, g_orc, f_gpu, f_orc, exact=True):
+    assert g_gpu.shape == g_orc.shape
+    rl = per_trace_rel_l2(g_gpu, g_orc)
+    assert rl.max() <= TOL, f"gather: max per-trace rel L2 {rl.max():.3e}"
+    for f in FIELDS:
+        num = np.linalg.norm((f_gpu[f] - f_orc[f]).astype(np.float64))
+        den = max(np.linalg.norm(f_orc[f].astype(np.float64)), 1e-30)
+        assert num / den <= TOL, f"field {f}: rel L2 {num / den:.3e}"
+    if exact:
+        diff = np.abs(g_gpu - g_orc).max() if g_gpu.size else 0.0
+        assert np.array_equal(g_gpu, g_orc), f"gather not bit-identical (max abs diff {diff:.3e})"
+        for f in FIELDS:
+            assert np.array_equal(f_gpu[f], f_orc[f]), f"field {f} not bit-identical"
+
+
+def _band_source_case():
+    # source inside the left HABC band and the bottom band (bottom-left corner)
+    c = layered(38, 30, seed=11, nbc=6, fd_order=8, nt=140)
+    M = 4
+    c.src_x = -float(c.dx) * (M + 2)                 # i = nbc - 1
+    c.src_z = float(c.dz) * (c.vp.shape[1] + M + 1)  # j inside the bottom band
+    c.name += "_bandsrc"
+    return c
+
+
+def _right_band_source_case():
+    c = layered(35, 28, seed=12, nbc=9, fd_order=4, nt=140, free_surface=False, rec_type="p")
+    c.src_x = float(c.dx) * (c.vp.shape[0] + 3)      # right HABC band
+    c.src_z = float(c.dz) * 4
+    c.name += "_rightsrc"
+    return c
+
+
+CASES = [
+    layered(40, 30, seed=1, nbc=6, fd_order=8, nt=150),
+    layered(37, 33, seed=2, nbc=5, fd_order=4, nt=150, rec_type="vx"),
+    layered(41, 27, seed=3, nbc=7, fd_order=12, nt=120, rec_type="p", water_rows=3),
+    layered(36, 31, seed=4, nbc=6, fd_order=8, free_surface=False, nt=150),
+    layered(35, 30, seed=5, nbc=8, fd_order=2, nt=100, free_surface=False, rec_type="p"),
+    layered(45, 26, seed=6, nbc=13, fd_order=6, nt=110),
+    layered(33, 34, seed=7, nbc=16, fd_order=10, nt=90, free_surface=False, rec_type="vx"),
+    layered(50, 22, seed=8, nbc=17, fd_order=8, nt=90, water_rows=2),
+    _band_source_case(),
+    _right_band_source_case(),
+]
+
+
+@pytest.mark.parametrize("c", CASES, ids=lambda c: c.name)
+def test_shot_matches_oracle(c, b200, oracle_lib):
+    r, f_gpu = gpu_run(c, b200)
+    g_orc, f_orc = oracle_run(c, oracle_lib)
+    assert_same(r.gather, g_orc, f_gpu, f_orc)
+    assert r.stats["steps"] == c.nt
+
+
+def test_shot_1_golden(b200, oracle_lib):
+    c = runjl_case()
+    r, f_gpu = gpu_run(c, b200)
+    ref = golden_gather()
+    rl = per_trace_rel_l2(r.gather, ref)
+    assert rl.max() <= TOL, f"vs shot_1.bin: max per-trace rel L2 {rl.max():.3e}"
+    g_orc, f_orc = oracle_run(c, oracle_lib)
+    assert_same(r.gather, g_orc, f_gpu, f_orc)
+
+
+def test_on_step_chunks_and_early_stop(b200, oracle_lib):
+    c = layered(39, 29, seed=21, nbc=6, fd_order=8, nt=130, rec_type="p")
+    full, f_full = gpu_run(c, b200)
+    seen = []
+    chunked, f_chunk = gpu_run(c, b200, on_step=lambda W, info: seen.append(info.k), step_chunk=37)
+    assert seen == [37, 74, 111, 130]
+    assert np.array_equal(full.gather, chunked.gather)
+    for f in FIELDS:
+        assert np.array_equal(f_full[f], f_chunk[f])
+    stop_at = 50
+    early, f_early = gpu_run(c, b200, on_step=lambda W, info: info.k < stop_at, step_chunk=25)
+    g_orc, f_orc = oracle_run(c, oracle_lib, n_steps=stop_at)
+    assert_same(early.gather, g_orc, f_early, f_orc)
+    assert not early.gather[stop_at:].any()
+
+
+def test_wavefield_reused_across_shots(b200):
+    c = layered(30, 24, seed=31, nbc=5, fd_order=8, nt=80)
+    W = None
+    med = F.init_medium(c.vp, c.vs, c.rho, c.dx, c.dz, c.nbc, c.fd_order, b200)
+    W = F.Wavefield(med.nx, med.nz, b200)
+    r1, _ = gpu_run(c, b200, W=W)
+    r2, _ = gpu_run(c, b200, W=W)
+    assert np.array_equal(r1.gather, r2.gather)
+    W.release()
+    med.release()
+
+
+def test_invalid_inputs_raise(b200):
+    c = layered(30, 24, seed=41, nbc=5, fd_order=8, nt=20)
+    c.rec_x = np.array([1e6], dtype=np.float32)
+    c.rec_z = np.array([0.0], dtype=np.float32)
+    with pytest.raises(F._lib.FomoError, match="FOMO_EINVAL.*receiver"):
+        gpu_run(c, b200)

@@ -285,18 +285,21 @@ def b200_arm(args, rank, world, local):
     for _ in range(args.warmup):
         device_shot()
     with ClockSampler(local) as clk:
-        ms, launches, _ = timed(device_shot, args.steps)
+        ms, launches, st_v = timed(device_shot, args.steps)
     clocks = clk.summary()
     value = world * args.steps * cells * w.nt / (ms / 1e3) / 1e9
 
     e2e = None
     if not args.no_e2e:
         e2e_shot()
-        ms_e, _, st_e = timed(e2e_shot, args.steps)
+        with ClockSampler(local) as clk_e:
+            ms_e, _, st_e = timed(e2e_shot, args.steps)
         h2d = sum(t.numel() * 4 for t in pinned) + st_e[0].h2d_bytes
         e2e = {"value": world * args.steps * cells * w.nt / (ms_e / 1e3) / 1e9, "unit": METRIC,
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(st_e[0].d2h_bytes),
                "ms_per_step": ms_e / args.steps,
+               "loop_ms_per_shot": [round(t.device_ms, 2) for t in st_e],
+               "clocks": clk_e.summary(),
                "path": "fomo_b200_medium_create + fomo_b200_run_shot (pinned host buffers) + medium_destroy"}
 
     # roofline of the dominant kernel: CUDA events around each launch
@@ -352,6 +355,7 @@ def b200_arm(args, rank, world, local):
                        "shots_per_gpu_per_step": 1, "parallelism": f"shot-sharded x{world}",
                        "l2": "inputs larger than L2 (357 MB medium + 715 MB state per shot)",
                        "bytes_per_cell_step_algorithmic": 60},
+            "loop_ms_per_shot": [round(t.device_ms, 2) for t in st_v],
             "e2e": e2e, "gpu_launches": int(launches), "clocks": clocks, "roofline": roofline,
             "cpu_baseline": cpu,
         }

@@ -3,6 +3,8 @@
 // Owns every device allocation behind opaque handles, one CUDA stream per
 // process, and the time loop of a shot.  See include/fomo_b200.h for the
 // reference interface each entry point stands in for.
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -16,7 +18,7 @@
 #include <vector>
 
 #include "../../include/fomo_b200.h"
-#include "step_simple.cuh"
+#include "step_tiled.cuh"
 
 namespace {
 
@@ -58,9 +60,18 @@ struct Medium : Object {
     int nx = 0, nz = 0, pitch = 0, M = 0, pad = 0, fs = 0;
     float dx = 0, dz = 0;
     float* base = nullptr;  // 5 arrays of pitch*nz floats
+    // Buoyancy dtx/rho_vx, dtz/rho_vx, dtx/rho_vz, dtz/rho_vz for the last
+    // (dtx, dtz) used; when dtx == dtz the second and fourth alias the first
+    // and third.
+    float* buoy = nullptr;
+    float buoy_dtx = 0, buoy_dtz = 0;
+    bool maps_ok = false;
+    CUtensorMap mod_maps[3];   // tile boxes of lam, mu_txx, mu_txz
+    CUtensorMap buoy_maps[4];  // tile boxes of the four buoyancy arrays
     const float* arr(int q) const { return base + (size_t)q * pitch * nz; }
     ~Medium() override {
         if (base) cudaFree(base);
+        if (buoy) cudaFree(buoy);
     }
 };
 
@@ -68,6 +79,9 @@ struct Wavefield : Object {
     int nx = 0, nz = 0, pitch = 0;
     float* base = nullptr;  // 2 copies x 5 fields of pitch*nz floats
     int cur = 0;            // copy holding the current state
+    int map_M = 0;          // M the halo maps were made for (0 = none)
+    CUtensorMap maps[2][5]; // halo boxes (Geo<map_M>) of every field of both copies
+    CUtensorMap pmaps[2][5];// tile boxes of every field of both copies
     float* field(int copy, int q) const { return base + ((size_t)copy * 5 + q) * pitch * nz; }
     ~Wavefield() override {
         if (base) cudaFree(base);
@@ -102,6 +116,7 @@ struct Context {
     int device = -1;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    int* d_status = nullptr;   // device error word of the kernels
     uint64_t next = 1;
     std::unordered_map<uint64_t, std::unique_ptr<Object>> objs;
 };
@@ -139,24 +154,105 @@ int check_medium_args(int nx, int nz, int M, int pad) {
     return FOMO_OK;
 }
 
-// Launch shape of one half step.
+// ---------------------------------------------------------------- TMA descriptors
+PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
+
+int get_encode() {
+    if (g_encode) return FOMO_OK;
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    CUDA_TRY(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q));
+    if (q != cudaDriverEntryPointSuccess || !fn) return fail(FOMO_ECUDA, "cuTensorMapEncodeTiled not available");
+    g_encode = (PFN_cuTensorMapEncodeTiled_v12000)fn;
+    return FOMO_OK;
+}
+
+// 2-D Float32 descriptor of an (nx, nz) array with row pitch `pitch` floats;
+// out-of-range elements of a box read as zero.
+int encode_map(CUtensorMap* map, const float* base, int nx, int nz, int pitch, int boxw, int boxh) {
+    if (int rc = get_encode()) return rc;
+    cuuint64_t dims[2] = {(cuuint64_t)nx, (cuuint64_t)nz};
+    cuuint64_t strides[1] = {(cuuint64_t)pitch * sizeof(float)};
+    cuuint32_t box[2] = {(cuuint32_t)boxw, (cuuint32_t)boxh};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult r = g_encode(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, (void*)base, dims, strides, box, estr,
+                          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                          CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return fail(FOMO_ECUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+    return FOMO_OK;
+}
+
+template <int M>
+int make_maps(Wavefield& w) {
+    using G = fomo::Geo<M>;
+    for (int c = 0; c < 2; ++c)
+        for (int q = 0; q < 5; ++q) {
+            if (int rc = encode_map(&w.maps[c][q], w.field(c, q), w.nx, w.nz, w.pitch, G::BOXW, G::BOXH)) return rc;
+            if (int rc = encode_map(&w.pmaps[c][q], w.field(c, q), w.nx, w.nz, w.pitch, fomo::kTX, fomo::kTZ))
+                return rc;
+        }
+    w.map_M = M;
+    return FOMO_OK;
+}
+
+int make_medium_maps(Medium& m) {
+    if (m.maps_ok) return FOMO_OK;
+    for (int q = 0; q < 3; ++q)
+        if (int rc = encode_map(&m.mod_maps[q], m.arr(2 + q), m.nx, m.nz, m.pitch, fomo::kTX, fomo::kTZ)) return rc;
+    m.maps_ok = true;
+    return FOMO_OK;
+}
+
+// ---------------------------------------------------------------- buoyancy
+int ensure_buoyancy(Medium& m, float dtx, float dtz) {
+    if (m.buoy && m.buoy_dtx == dtx && m.buoy_dtz == dtz) return FOMO_OK;
+    const size_t plane = (size_t)m.pitch * m.nz;
+    if (!m.buoy) {
+        cudaError_t e = cudaMalloc(&m.buoy, 4 * plane * sizeof(float));
+        if (e != cudaSuccess) return fail(FOMO_ENOMEM, "buoyancy allocation failed: %s", cudaGetErrorString(e));
+    }
+    float* b0 = m.buoy;
+    float* b1 = dtx == dtz ? b0 : m.buoy + plane;
+    float* b2 = m.buoy + 2 * plane;
+    float* b3 = dtx == dtz ? b2 : m.buoy + 3 * plane;
+    fomo::buoyancy_kernel<<<4 * 148, 256, 0, ctx().stream>>>(m.arr(0), m.arr(1), dtx, dtz, plane, b0, b1, b2, b3);
+    CUDA_TRY(cudaGetLastError());
+    m.buoy_dtx = dtx;
+    m.buoy_dtz = dtz;
+    const float* bp[4] = {b0, b1, b2, b3};
+    for (int q = 0; q < 4; ++q)
+        if (int rc = encode_map(&m.buoy_maps[q], bp[q], m.nx, m.nz, m.pitch, fomo::kTX, fomo::kTZ)) return rc;
+    return FOMO_OK;
+}
+
+void buoyancy_ptrs(const Medium& m, const float* out[4]) {
+    const size_t plane = (size_t)m.pitch * m.nz;
+    out[0] = m.buoy;
+    out[1] = m.buoy_dtx == m.buoy_dtz ? m.buoy : m.buoy + plane;
+    out[2] = m.buoy + 2 * plane;
+    out[3] = m.buoy_dtx == m.buoy_dtz ? m.buoy + 2 * plane : m.buoy + 3 * plane;
+}
+
+// ---------------------------------------------------------------- launches
 struct Launch {
-    int tiles_x, tiles_z, n_tile, n_band;
-    size_t band_smem_v, band_smem_s;
+    int tiles_x, tiles_z, n_tile, n_band, x_last;
+    size_t smem_v, smem_s;
 };
 
-Launch launch_shape(int nx, int nz, int nbc) {
+template <int M>
+Launch launch_shape(int nx, int nz, int nbc, bool iso) {
     Launch L;
-    L.tiles_x = (nx + fomo::kTileX - 1) / fomo::kTileX;
-    L.tiles_z = (nz + fomo::kTileZ - 1) / fomo::kTileZ;
+    L.tiles_x = (nx + fomo::kTX - 1) / fomo::kTX;
+    L.tiles_z = (nz + fomo::kTZ - 1) / fomo::kTZ;
+    L.x_last = std::max(0, (nx + 3) / 4 * 4 - fomo::kTX);  // last tile ends at the grid's right edge
     L.n_tile = L.tiles_x * L.tiles_z;
     L.n_band = (nx + fomo::kBandW - 1) / fomo::kBandW;
-    L.band_smem_v = 4 * (size_t)2 * ((size_t)(nbc + 1) * (fomo::kBandW + 6) + 2 * (fomo::kBandW + 2));
-    L.band_smem_s = 4 * (size_t)3 * ((size_t)(nbc + 1) * (fomo::kBandW + 6) + 2 * (fomo::kBandW + 2));
+    L.smem_v = fomo::tiled_smem_bytes<M>(true, nbc, iso);
+    L.smem_s = fomo::tiled_smem_bytes<M>(false, nbc, iso);
     return L;
 }
 
-void fill_common(fomo::StepParams& P, const Medium& m, const Shot& s, const Launch& L) {
+void fill_common(fomo::StepParams& P, const Medium& m, const Shot& s) {
     std::memset(&P, 0, sizeof(P));
     P.nx = m.nx;
     P.nz = m.nz;
@@ -186,10 +282,6 @@ void fill_common(fomo::StepParams& P, const Medium& m, const Shot& s, const Laun
     P.rec_kind = s.rec_kind;
     P.rec_cell = s.d_rec;
     P.gather = s.d_gather;
-    P.tiles_x = L.tiles_x;
-    P.tiles_z = L.tiles_z;
-    P.n_tile_blocks = L.n_tile;
-    P.n_band_blocks = L.n_band;
 }
 
 // Per-launch event pairs, filled only by fomo_b200_shot_profile.
@@ -210,51 +302,88 @@ struct Profile {
     }
 };
 
-int run_steps(Shot& s, int n_steps, Profile* prof = nullptr) {
+int check_status() {
+    int st = 0;
+    CUDA_TRY(cudaMemcpyAsync(&st, ctx().d_status, sizeof(int), cudaMemcpyDeviceToHost, ctx().stream));
+    CUDA_TRY(cudaStreamSynchronize(ctx().stream));
+    if (st == fomo::kErrTmaTimeout) return fail(FOMO_ETIMEOUT, "a TMA load of a time-step kernel did not complete");
+    if (st) return fail(FOMO_ECUDA, "time-step kernel reported error %d", st);
+    return FOMO_OK;
+}
+
+template <int M>
+int run_steps_M(Shot& s, Medium& m, Wavefield& w, int n_steps, Profile* prof) {
     auto& C = ctx();
-    Medium* m = get<Medium>(s.medium);
-    Wavefield* w = get<Wavefield>(s.wavefield);
-    if (!m || !w) return fail(FOMO_EINVAL, "shot refers to a destroyed medium or wavefield");
-    const Launch L = launch_shape(m->nx, m->nz, s.nbc);
-    static size_t smem_set_v = 0, smem_set_s = 0;
-    if (L.band_smem_v > 48 * 1024 && L.band_smem_v > smem_set_v) {
-        CUDA_TRY(cudaFuncSetAttribute(fomo::velocity_simple_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)L.band_smem_v));
-        smem_set_v = L.band_smem_v;
+    const bool iso = s.dtx == s.dtz;
+    const Launch L = launch_shape<M>(m.nx, m.nz, s.nbc, iso);
+    static size_t smem_set_v = 48 * 1024, smem_set_s = 48 * 1024;
+    if (L.smem_v > smem_set_v) {
+        CUDA_TRY(cudaFuncSetAttribute(fomo::velocity_kernel<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.smem_v));
+        smem_set_v = L.smem_v;
     }
-    if (L.band_smem_s > 48 * 1024 && L.band_smem_s > smem_set_s) {
-        CUDA_TRY(cudaFuncSetAttribute(fomo::stress_simple_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)L.band_smem_s));
-        smem_set_s = L.band_smem_s;
+    if (L.smem_s > smem_set_s) {
+        CUDA_TRY(cudaFuncSetAttribute(fomo::stress_kernel<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.smem_s));
+        smem_set_s = L.smem_s;
     }
-    const int rec_blocks = (s.n_rec + 255) / 256;
+    if (w.map_M != M)
+        if (int rc = make_maps<M>(w)) return rc;
+    if (int rc = ensure_buoyancy(m, s.dtx, s.dtz)) return rc;
+    if (int rc = make_medium_maps(m)) return rc;
+    fomo::TiledArgs T;
+    buoyancy_ptrs(m, T.b);
+    T.iso = iso ? 1 : 0;
+    T.status = C.d_status;
+    T.n_band_blocks = L.n_band;
+    T.n_tile_blocks = L.n_tile;
+    T.tiles_x = L.tiles_x;
+    T.x_last = L.x_last;
+    const int rec_blocks = (s.n_rec + fomo::kThreads - 1) / fomo::kThreads;
     CUDA_TRY(cudaEventRecord(C.ev0, C.stream));
     const int k_end = std::min(s.nt, s.k_done + n_steps);
     for (int k = s.k_done + 1; k <= k_end; ++k) {
-        const int a = w->cur, b = 1 - w->cur;
+        const int a = w.cur, b = 1 - w.cur;
         fomo::StepParams P;
-        fill_common(P, *m, s, L);
+        fill_common(P, m, s);
         P.src_w = (k <= (int)s.wavelet.size()) ? s.wavelet[k - 1] : 0.f;
         // velocity: reads v(a), tau(a); writes v(b); records step k-1 from copy a
-        for (int q = 0; q < 5; ++q) P.in[q] = w->field(a, q);
-        P.out[fomo::VX] = w->field(b, fomo::VX);
-        P.out[fomo::VZ] = w->field(b, fomo::VZ);
+        for (int q = 0; q < 5; ++q) P.in[q] = w.field(a, q);
+        P.out[fomo::VX] = w.field(b, fomo::VX);
+        P.out[fomo::VZ] = w.field(b, fomo::VZ);
         P.rec_k = (k >= 2 && s.n_rec > 0) ? k - 1 : 0;
-        const int vblocks = L.n_tile + L.n_band + (P.rec_k ? rec_blocks : 0);
+        const int vblocks = L.n_band + L.n_tile + (P.rec_k ? rec_blocks : 0);
         if (prof && prof->add(C.stream, 0)) return fail(FOMO_ECUDA, "profiling event failed");
-        fomo::velocity_simple_kernel<<<vblocks, 256, L.band_smem_v, C.stream>>>(P);
+        fomo::VelMaps vm;
+        vm.xx = w.maps[a][fomo::TXX];
+        vm.zz = w.maps[a][fomo::TZZ];
+        vm.xz = w.maps[a][fomo::TXZ];
+        vm.vx = w.pmaps[a][fomo::VX];
+        vm.vz = w.pmaps[a][fomo::VZ];
+        vm.b0 = m.buoy_maps[0];
+        vm.b1 = m.buoy_maps[1];
+        vm.b2 = m.buoy_maps[2];
+        vm.b3 = m.buoy_maps[3];
+        fomo::velocity_kernel<M><<<vblocks, fomo::kThreads, L.smem_v, C.stream>>>(P, T, vm);
         if (prof && prof->end(C.stream)) return fail(FOMO_ECUDA, "profiling event failed");
         // stress: reads v(b) (new), tau(a); writes tau(b)
-        P.in[fomo::VX] = w->field(b, fomo::VX);
-        P.in[fomo::VZ] = w->field(b, fomo::VZ);
-        for (int q = 2; q < 5; ++q) P.out[q] = w->field(b, q);
+        P.in[fomo::VX] = w.field(b, fomo::VX);
+        P.in[fomo::VZ] = w.field(b, fomo::VZ);
+        for (int q = 2; q < 5; ++q) P.out[q] = w.field(b, q);
         P.out[fomo::VX] = P.out[fomo::VZ] = nullptr;
         P.rec_k = 0;
         if (prof && prof->add(C.stream, 1)) return fail(FOMO_ECUDA, "profiling event failed");
-        fomo::stress_simple_kernel<<<L.n_tile + L.n_band, 256, L.band_smem_s, C.stream>>>(P);
+        fomo::StrMaps sm;
+        sm.vx = w.maps[b][fomo::VX];
+        sm.vz = w.maps[b][fomo::VZ];
+        sm.txx = w.pmaps[a][fomo::TXX];
+        sm.tzz = w.pmaps[a][fomo::TZZ];
+        sm.txz = w.pmaps[a][fomo::TXZ];
+        sm.lam = m.mod_maps[0];
+        sm.mu = m.mod_maps[1];
+        sm.mxz = m.mod_maps[2];
+        fomo::stress_kernel<M><<<L.n_band + L.n_tile, fomo::kThreads, L.smem_s, C.stream>>>(P, T, sm);
         if (prof && prof->end(C.stream)) return fail(FOMO_ECUDA, "profiling event failed");
         s.launches += 2;
-        w->cur = b;
+        w.cur = b;
         if (k >= 2) s.recorded = k - 1;
         s.k_done = k;
     }
@@ -264,7 +393,22 @@ int run_steps(Shot& s, int n_steps, Profile* prof = nullptr) {
     float ms = 0;
     CUDA_TRY(cudaEventElapsedTime(&ms, C.ev0, C.ev1));
     s.device_ms += ms;
-    return FOMO_OK;
+    return check_status();
+}
+
+int run_steps(Shot& s, int n_steps, Profile* prof = nullptr) {
+    Medium* m = get<Medium>(s.medium);
+    Wavefield* w = get<Wavefield>(s.wavefield);
+    if (!m || !w) return fail(FOMO_EINVAL, "shot refers to a destroyed medium or wavefield");
+    switch (m->M) {
+        case 1: return run_steps_M<1>(s, *m, *w, n_steps, prof);
+        case 2: return run_steps_M<2>(s, *m, *w, n_steps, prof);
+        case 3: return run_steps_M<3>(s, *m, *w, n_steps, prof);
+        case 4: return run_steps_M<4>(s, *m, *w, n_steps, prof);
+        case 5: return run_steps_M<5>(s, *m, *w, n_steps, prof);
+        case 6: return run_steps_M<6>(s, *m, *w, n_steps, prof);
+    }
+    return fail(FOMO_EINVAL, "M=%d not supported", m->M);
 }
 
 // Records the receivers of the last step done (the next velocity launch would).
@@ -274,12 +418,11 @@ int record_last(Shot& s) {
     Medium* m = get<Medium>(s.medium);
     Wavefield* w = get<Wavefield>(s.wavefield);
     if (!m || !w) return fail(FOMO_EINVAL, "shot refers to a destroyed medium or wavefield");
-    const Launch L = launch_shape(m->nx, m->nz, s.nbc);
     fomo::StepParams P;
-    fill_common(P, *m, s, L);
+    fill_common(P, *m, s);
     for (int q = 0; q < 5; ++q) P.in[q] = w->field(w->cur, q);
     P.rec_k = s.k_done;
-    fomo::record_kernel<<<(s.n_rec + 255) / 256, 256, 0, C.stream>>>(P);
+    fomo::record_kernel<<<(s.n_rec + fomo::kThreads - 1) / fomo::kThreads, fomo::kThreads, 0, C.stream>>>(P);
     CUDA_TRY(cudaGetLastError());
     s.launches += 1;
     s.recorded = s.k_done;
@@ -311,6 +454,8 @@ int fomo_b200_init(int device) {
     CUDA_TRY(cudaStreamCreateWithFlags(&C.stream, cudaStreamNonBlocking));
     CUDA_TRY(cudaEventCreate(&C.ev0));
     CUDA_TRY(cudaEventCreate(&C.ev1));
+    CUDA_TRY(cudaMalloc(&C.d_status, sizeof(int)));
+    CUDA_TRY(cudaMemset(C.d_status, 0, sizeof(int)));
     C.device = device;
     C.inited = true;
     return FOMO_OK;
@@ -324,6 +469,8 @@ int fomo_b200_shutdown(void) {
     C.objs.clear();
     cudaEventDestroy(C.ev0);
     cudaEventDestroy(C.ev1);
+    cudaFree(C.d_status);
+    C.d_status = nullptr;
     cudaStreamDestroy(C.stream);
     C.stream = nullptr;
     C.inited = false;
@@ -584,6 +731,7 @@ int fomo_b200_shot_begin(uint64_t medium, uint64_t wavefield, const FomoHabc* ha
     }
     s->h2d += (int64_t)s->wavelet.size() * 4;
     if (int rc = wavefield_reset_locked(w)) return rc;
+    CUDA_TRY(cudaMemsetAsync(ctx().d_status, 0, sizeof(int), st));
     CUDA_TRY(cudaStreamSynchronize(st));
     *shot_handle = put(std::move(s));
     return FOMO_OK;

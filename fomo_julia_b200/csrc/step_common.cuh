@@ -61,13 +61,24 @@ __device__ __forceinline__ size_t cell(const StepParams& P, int i, int j) {
     return (size_t)i + (size_t)j * (size_t)P.pitch;
 }
 
+// P.in[q] for a q known only at run time, written as selects so the
+// parameter block is not copied to local memory.
+__device__ __forceinline__ const float* in_field(const StepParams& P, int q) {
+    const float* p = P.in[0];
+    p = q == 1 ? P.in[1] : p;
+    p = q == 2 ? P.in[2] : p;
+    p = q == 3 ? P.in[3] : p;
+    p = q == 4 ? P.in[4] : p;
+    return p;
+}
+
 // ---------------------------------------------------------------------------
 // Stencils.  The explosive source (txx, tzz += w at the source cell,
 // source_receiver.jl:26-27) is applied to the values read, never stored, so
 // the stored fields keep the pre-injection values the HABC needs as f_old.
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ float tau_in(const StepParams& P, int q, int i, int j) {
-    float v = __ldg(P.in[q] + cell(P, i, j));
+    float v = __ldg(in_field(P, q) + cell(P, i, j));
     if (q != TXZ && i == P.src_i && j == P.src_j) v = fadd(v, P.src_w);
     return v;
 }

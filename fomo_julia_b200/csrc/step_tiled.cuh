@@ -1,0 +1,839 @@
+// step_tiled.cuh -- the sm_100a time-step kernels (one launch per half step).
+//
+// Data flow per half step (velocity: reads tau, writes v; stress: reads the
+// new v, writes tau).  The step reads the five fields from one copy of the
+// wavefield and writes the other copy, so every written cell is a pure
+// function of read-only inputs and no ordering is needed inside a launch.
+// Block roles of one launch, in launch order:
+//
+//   [0, n_band)              bottom band: rows nz-nbc-1..nz-2 (bottom edge and
+//                            corners), kBandW columns per block; the HABC
+//                            recurrence along j runs down the band in shared
+//                            memory.  First in the grid so their serial part
+//                            overlaps the tiles.
+//   [n_band, +n_tiles)       64 x 16 cell tiles in raster order; the last tile
+//                            of a row is aligned to the right edge of the grid
+//                            so that the right HABC band and the two columns
+//                            its rules read lie in one tile, as the left band
+//                            does in the first tile.
+//       fast tiles: the stencil fields of the tile plus an M-cell halo and
+//         the tile's pointwise operands arrive by TMA (cp.async.bulk.tensor.2d,
+//         one mbarrier); each thread owns 4 columns x 2 rows, forms
+//         x-derivatives from 128-bit shared-memory row windows and
+//         z-derivatives from a (2M+1)-row register window.  Tiles
+//         holding left/right HABC cells park their stencil values in shared
+//         memory and apply the HABC rules of step_common.cuh to them.
+//       generic tiles (top HABC band without a free surface, or HABC bands
+//         wider than a tile allows): stencil values of the tile plus a 4 x 2
+//         margin are computed into shared memory cell by cell, then the rules.
+//   [.., +record blocks)     receivers of step rec_k (velocity launch only).
+#pragma once
+
+#include <cuda.h>
+
+#include "step_common.cuh"
+
+namespace fomo {
+
+constexpr int kTX = 64, kTZ = 16, kThreads = 128;
+constexpr int kCG = kTX / 4;   // float4 column groups of a tile row
+constexpr int kBandW = 16;
+constexpr int kEdgeX = 4, kEdgeZ = 2;  // margin of stencil values around an edge tile
+
+template <int M>
+struct Geo {
+    static constexpr int HQ = (M + 3) / 4;          // float4s of x halo on each side
+    static constexpr int HX = 4 * HQ;               // x halo of the TMA box (16-byte aligned)
+    static constexpr int BOXW = kTX + 2 * HX;
+    static constexpr int BOXH = kTZ + 2 * M;
+    static constexpr int NQ = 1 + 2 * HQ;           // float4s of an x window
+    static constexpr int BOXS = (BOXW * BOXH + 31) / 32 * 32;  // floats per box in smem (128-byte multiple)
+    static constexpr int RW = kTX + 2 * kEdgeX, RH = kTZ + 2 * kEdgeZ;  // edge-tile value region
+};
+constexpr int kPBox = kTX * kTZ;  // floats of a pointwise box (the tile itself, no halo)
+
+// Device-side parameters beyond StepParams.
+struct TiledArgs {
+    const float* b[4];   // buoyancy dtx/rho_vx, dtz/rho_vx, dtx/rho_vz, dtz/rho_vz
+    int iso;             // dtx == dtz: b[1] == b[0] and b[3] == b[2]
+    int* status;         // first nonzero error code of the launch (0 = ok)
+    int n_band_blocks, n_tile_blocks, tiles_x;
+    int x_last;          // first column of the last tile of a row (a multiple of 4)
+};
+
+__device__ __forceinline__ int tile_x0(const TiledArgs& T, int tx) {
+    return tx == T.tiles_x - 1 ? T.x_last : tx * kTX;
+}
+
+// Column-pair arithmetic: two scalar IEEE round-to-nearest operations.  The
+// sm_100a paired FP32 instructions (add/mul/sub.rn.f32x2, and the
+// __fadd2_rn/__fmul2_rn intrinsics) were measured to give results that are
+// not bit-identical to these scalar operations on this path, so the kernels
+// keep the scalar forms and stay bit-identical to the CPU evaluation.
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return make_float2(fadd(a.x, b.x), fadd(a.y, b.y)); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return make_float2(fmul(a.x, b.x), fmul(a.y, b.y)); }
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return make_float2(fsub(a.x, b.x), fsub(a.y, b.y)); }
+__device__ __forceinline__ float2 lo2(const float4& v) { return make_float2(v.x, v.y); }
+__device__ __forceinline__ float2 hi2(const float4& v) { return make_float2(v.z, v.w); }
+
+// TMA descriptors of one launch.  Velocity: halo boxes of txx, tzz, txz;
+// tile boxes of vx, vz, b0..b3.  Stress: halo boxes of vx, vz; tile boxes of
+// txx, tzz, txz, lam, mu_txx, mu_txz.
+struct VelMaps {
+    CUtensorMap xx, zz, xz, vx, vz, b0, b1, b2, b3;
+};
+struct StrMaps {
+    CUtensorMap vx, vz, txx, tzz, txz, lam, mu, mxz;
+};
+
+constexpr int kErrTmaTimeout = 1;
+
+// ---------------------------------------------------------------- PTX helpers
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void fence_barrier_init() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// 2-D tiled TMA load of box (x, z) of `map` into shared memory, completing on `bar`.
+__device__ __forceinline__ void tma_load_2d(float* dst, const CUtensorMap* map, int x, int z, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
+        ::"r"(smem_u32(dst)), "l"((uint64_t)map), "r"(x), "r"(z), "r"(smem_u32(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ float4 ldg4(const float* p) { return __ldg(reinterpret_cast<const float4*>(p)); }
+__device__ __forceinline__ void stg4(float* p, float4 v) { *reinterpret_cast<float4*>(p) = v; }
+__device__ __forceinline__ float4 lds4(const float* p) { return *reinterpret_cast<const float4*>(p); }
+
+__device__ __forceinline__ float comp(const float4& v, int c) {
+    return c == 0 ? v.x : (c == 1 ? v.y : (c == 2 ? v.z : v.w));
+}
+__device__ __forceinline__ void set_comp(float4& v, int c, float x) {
+    if (c == 0) v.x = x; else if (c == 1) v.y = x; else if (c == 2) v.z = x; else v.w = x;
+}
+
+// Waits for the TMA boxes of this block; false (and status set) on timeout.
+__device__ __forceinline__ bool wait_tma(uint64_t* bar, const TiledArgs& T) {
+    for (int it = 0; it < (1 << 24); ++it)
+        if (mbar_try_wait(bar, 0)) return true;
+    atomicCAS(T.status, 0, kErrTmaTimeout);
+    return false;
+}
+
+// Rows a tile stores: inside the grid and outside the bottom band (the band
+// blocks write whole band rows).
+__device__ __forceinline__ bool row_stored(const StepParams& P, int j) {
+    return j < P.nz && !(j >= P.nz - P.nbc - 1 && j <= P.nz - 2);
+}
+
+__device__ __forceinline__ bool lr_band_cell(const StepParams& P, int i, int j) {
+    const int js0 = P.fs ? P.nbc : 1;
+    return (i <= P.nbc || i >= P.nx - P.nbc - 1) && j >= js0 && j <= P.nz - P.nbc - 2;
+}
+
+// ---------------------------------------------------------------- shared-memory stencil values
+// Stencil input fields of one half step over [xa-M, xa+W+M) x [za-M, za+H+M)
+// into `sin` (field-major, row-major), zero outside the grid.  Velocity:
+// txx, tzz, txz with the source injected; stress: vx, vz.
+template <int M, bool VEL>
+__device__ void load_region_inputs(const StepParams& P, int xa, int za, int W, int H, float* sin) {
+    const int IW = W + 2 * M, IH = H + 2 * M;
+    constexpr int NF = VEL ? 3 : 2;
+    const int n = NF * IW * IH;
+    for (int idx = threadIdx.x; idx < n; idx += blockDim.x) {
+        const int f = idx / (IW * IH), r = idx - f * (IW * IH);
+        const int zz = r / IW, xx = r - zz * IW;
+        const int i = xa - M + xx, j = za - M + zz;
+        float v = 0.f;
+        if (i >= 0 && i < P.nx && j >= 0 && j < P.nz)
+            v = VEL ? tau_in(P, TXX + f, i, j) : __ldg(in_field(P, VX + f) + cell(P, i, j));
+        sin[idx] = v;
+    }
+}
+
+// Values after the stencil update (before the HABC) of the half step's
+// output fields over [xa, xa+W) x [za, za+H) into `spre` (field-major).
+template <int M, bool VEL>
+__device__ void compute_region_pre(const StepParams& P, const TiledArgs& T, int xa, int za, int W, int H,
+                                   const float* sin, float* spre) {
+    const int IW = W + 2 * M, IH = H + 2 * M;
+    auto S = [&](int f, int i, int j) -> float { return sin[(f * IH + (j - za + M)) * IW + (i - xa + M)]; };
+    for (int idx = threadIdx.x; idx < W * H; idx += blockDim.x) {
+        const int zz = idx / W, xx = idx - zz * W;
+        const int i = xa + xx, j = za + zz;
+        if (i < 0 || i >= P.nx || j < 0 || j >= P.nz) {
+            spre[idx] = 0.f;
+            spre[W * H + idx] = 0.f;
+            if (!VEL) spre[2 * W * H + idx] = 0.f;
+            continue;
+        }
+        const size_t c = cell(P, i, j);
+        if (VEL) {
+            float vx = __ldg(P.in[VX] + c), vz = __ldg(P.in[VZ] + c);
+            if (in_stencil(P, i, j)) {
+                float d1 = 0.f, d2 = 0.f, d3 = 0.f, d4 = 0.f;
+#pragma unroll
+                for (int l = 1; l <= M; ++l) {
+                    const float al = P.a[l - 1];
+                    d1 = fadd(fmul(al, fsub(S(0, i + l - 1, j), S(0, i - l, j))), d1);
+                    d2 = fadd(fmul(al, fsub(S(2, i, j + l - 1), S(2, i, j - l))), d2);
+                    d3 = fadd(fmul(al, fsub(S(2, i + l, j), S(2, i - l + 1, j))), d3);
+                    d4 = fadd(fmul(al, fsub(S(1, i, j + l), S(1, i, j - l + 1))), d4);
+                }
+                vx = fadd(vx, fadd(fmul(__ldg(T.b[0] + c), d1), fmul(__ldg(T.b[1] + c), d2)));
+                vz = fadd(vz, fadd(fmul(__ldg(T.b[2] + c), d3), fmul(__ldg(T.b[3] + c), d4)));
+            }
+            spre[idx] = vx;
+            spre[W * H + idx] = vz;
+        } else {
+            float txx = tau_in(P, TXX, i, j), tzz = tau_in(P, TZZ, i, j), txz = __ldg(P.in[TXZ] + c);
+            if (in_stencil(P, i, j)) {
+                float dvxdx = 0.f, dvzdz = 0.f, dvxdz = 0.f, dvzdx = 0.f;
+#pragma unroll
+                for (int l = 1; l <= M; ++l) {
+                    const float al = P.a[l - 1];
+                    dvxdx = fadd(fmul(al, fsub(S(0, i + l, j), S(0, i - l + 1, j))), dvxdx);
+                    dvzdz = fadd(fmul(al, fsub(S(1, i, j + l - 1), S(1, i, j - l))), dvzdz);
+                    dvxdz = fadd(fmul(al, fsub(S(0, i, j + l), S(0, i, j - l + 1))), dvxdz);
+                    dvzdx = fadd(fmul(al, fsub(S(1, i + l - 1, j), S(1, i - l, j))), dvzdx);
+                }
+                const float lv = __ldg(P.lam + c), mv = __ldg(P.mu_txx + c), mxz = __ldg(P.mu_txz + c);
+                const float l2m = fadd(lv, fmul(2.f, mv));
+                const float ex = fmul(dvxdx, P.dtx), ez = fmul(dvzdz, P.dtz);
+                txx = fadd(txx, fadd(fmul(l2m, ex), fmul(lv, ez)));
+                tzz = fadd(tzz, fadd(fmul(lv, ex), fmul(l2m, ez)));
+                txz = fadd(txz, fmul(mxz, fadd(fmul(dvxdz, P.dtz), fmul(dvzdx, P.dtx))));
+            }
+            spre[idx] = txx;
+            spre[W * H + idx] = tzz;
+            spre[2 * W * H + idx] = txz;
+        }
+    }
+}
+
+// Reads field f of a value region in shared memory.
+struct SmemPre {
+    const float* spre;
+    int xa, za, W, H, f;
+    __device__ float operator()(int i, int j) const { return spre[(f * H + (j - za)) * W + (i - xa)]; }
+};
+
+// ---------------------------------------------------------------- bottom band
+// Rows nz-nbc-1 .. nz-2, columns 1 .. nx-2: the bottom edge and the two
+// bottom corners.  Stencil values of the block's columns (plus a 3-column
+// halo) and the row above the band are computed into shared memory; then one
+// thread per column marches down the rows.  In a row, the bottom edge,
+// bottom-left cells below nbc and bottom-right cells that are not chunk
+// starts read stencil values of row j and finals of row j-1 (phase A); the
+// last bottom-left column reads the bottom edge's final value at i+1 and a
+// bottom-right chunk start the final value at i-1 (phase B).
+template <int M, bool VEL>
+__device__ void band_block(const StepParams& P, const TiledArgs& T, int bblock, float* smem) {
+    constexpr int NF = VEL ? 2 : 3;
+    const int b = P.nbc, nx = P.nx, nz = P.nz;
+    const int R = b + 1;              // rows nz-b-2 .. nz-2
+    const int C = kBandW + 6;         // cols x0-3 .. x0+kBandW+2
+    const int CF = kBandW + 2;        // chain cols x0-1 .. x0+kBandW
+    const int x0 = bblock * kBandW;
+    const int j_top = nz - b - 2;
+    // [stencil inputs, later the step-start values][stencil values][two chain rows]
+    const int n_in = (VEL ? 3 : 2) * (C + 2 * M) * (R + 2 * M);
+    float* sin = smem;                                    // NF_in x (C+2M) x (R+2M)
+    float* Om = smem;                                     // NF x R x C, once sin is dead
+    float* Pm = smem + max(n_in, NF * R * C);             // NF x R x C
+    float* Fa = Pm + NF * R * C;                          // NF x CF
+    float* Fb = Fa + NF * CF;
+    const int fidx[3] = {VEL ? VX : TXX, VEL ? VZ : TZZ, TXZ};
+
+    load_region_inputs<M, VEL>(P, x0 - 3, j_top, C, R, sin);
+    __syncthreads();
+    compute_region_pre<M, VEL>(P, T, x0 - 3, j_top, C, R, sin, Pm);
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < NF * R * C; idx += blockDim.x) {
+        const int f = idx / (R * C), r = idx - f * (R * C);
+        const int rr = r / C, c = r - rr * C;
+        const int i = x0 - 3 + c, j = j_top + rr;
+        const int q = VEL ? VX + f : TXX + f;
+        Om[idx] = (i >= 0 && i < nx) ? __ldg(in_field(P, q) + cell(P, i, j)) : 0.f;
+    }
+    __syncthreads();
+
+    const float* tabs[3] = {P.w_tab[VEL ? 0 : 2], P.w_tab[VEL ? 1 : 2], P.w_tab[2]};
+    auto PV = [&](int f, int i, int j) -> float { return Pm[(f * R + (j - j_top)) * C + (i - x0 + 3)]; };
+    auto OV = [&](int f, int i, int j) -> float { return Om[(f * R + (j - j_top)) * C + (i - x0 + 3)]; };
+    auto Wt = [&](int f, int i, int j) -> float { return habc_w(tabs[f], b, nx, nz, i, j); };
+    const int r0 = nx - b - 1;
+
+    // Row nz-b-2: values after the edge loops.
+    for (int cc = threadIdx.x; cc < CF; cc += blockDim.x) {
+        const int i = x0 - 1 + cc, j = j_top;
+#pragma unroll
+        for (int f = 0; f < NF; ++f) {
+            float val = 0.f;
+            if (i >= 0 && i < nx) {
+                val = PV(f, i, j);
+                if (i >= 1 && i <= b) {
+                    val = blend_edge(Wt(f, i, j), PV(f, i, j),
+                                     edge_sum(P.qx, P.qt_x, P.qxt, PV(f, i + 1, j), OV(f, i, j), OV(f, i + 1, j)));
+                } else if (i >= r0 && i <= nx - 2) {
+                    auto rplain = [&](int ii) {
+                        return blend_edge(Wt(f, ii, j), PV(f, ii, j),
+                                          edge_sum(P.qx, P.qt_x, P.qxt, PV(f, ii - 1, j), OV(f, ii, j), OV(f, ii - 1, j)));
+                    };
+                    if (i > r0 && right_chunk_start(nx, b, i)) {
+                        val = blend_edge(Wt(f, i, j), PV(f, i, j),
+                                         edge_sum(P.qx, P.qt_x, P.qxt, rplain(i - 1), OV(f, i, j), OV(f, i - 1, j)));
+                    } else {
+                        val = rplain(i);
+                    }
+                }
+            }
+            Fa[f * CF + cc] = val;
+        }
+    }
+    __syncthreads();
+
+    float* Fprev = Fa;
+    float* Fcur = Fb;
+    for (int j = j_top + 1; j <= nz - 2; ++j) {
+        for (int cc = threadIdx.x; cc < CF; cc += blockDim.x) {
+            const int i = x0 - 1 + cc;
+            if (i < 0 || i >= nx) continue;
+            const bool phase_b = (i == b) || (i >= r0 && i <= nx - 2 && right_chunk_start(nx, b, i));
+            if (phase_b && i >= 1 && i <= nx - 2) continue;
+#pragma unroll
+            for (int f = 0; f < NF; ++f) {
+                float val;
+                const float own = PV(f, i, j);
+                if (i == 0 || i == nx - 1) {
+                    val = own;
+                } else if (i <= b) {  // bottom-left corner
+                    const float sx = edge_sum(P.qx, P.qt_x, P.qxt, PV(f, i + 1, j), OV(f, i, j), OV(f, i + 1, j));
+                    const float sz = edge_sum(P.qz, P.qt_z, P.qxt, Fprev[f * CF + cc], OV(f, i, j), OV(f, i, j - 1));
+                    val = blend_corner(Wt(f, i, j), own, sx, sz);
+                } else if (i >= r0) {  // bottom-right corner
+                    const float sx = edge_sum(P.qx, P.qt_x, P.qxt, PV(f, i - 1, j), OV(f, i, j), OV(f, i - 1, j));
+                    const float sz = edge_sum(P.qz, P.qt_z, P.qxt, Fprev[f * CF + cc], OV(f, i, j), OV(f, i, j - 1));
+                    val = blend_corner(Wt(f, i, j), own, sx, sz);
+                } else {  // bottom edge
+                    val = blend_edge(Wt(f, i, j), own,
+                                     edge_sum(P.qz, P.qt_z, P.qxt, Fprev[f * CF + cc], OV(f, i, j), OV(f, i, j - 1)));
+                }
+                Fcur[f * CF + cc] = val;
+            }
+        }
+        __syncthreads();
+        for (int cc = threadIdx.x; cc < CF; cc += blockDim.x) {
+            const int i = x0 - 1 + cc;
+            if (i < 1 || i > nx - 2) continue;
+            const bool bl_last = (i == b);
+            const bool br_start = (i >= r0 && right_chunk_start(nx, b, i));
+            if (!bl_last && !br_start) continue;
+            if (bl_last && cc + 1 >= CF) continue;  // halo column: value unused
+            if (br_start && cc == 0) continue;      // halo column: value unused
+#pragma unroll
+            for (int f = 0; f < NF; ++f) {
+                const float own = PV(f, i, j);
+                const int ix = bl_last ? i + 1 : i - 1;
+                const float fx = Fcur[f * CF + (bl_last ? cc + 1 : cc - 1)];
+                const float sx = edge_sum(P.qx, P.qt_x, P.qxt, fx, OV(f, i, j), OV(f, ix, j));
+                const float sz = edge_sum(P.qz, P.qt_z, P.qxt, Fprev[f * CF + cc], OV(f, i, j), OV(f, i, j - 1));
+                Fcur[f * CF + cc] = blend_corner(Wt(f, i, j), own, sx, sz);
+            }
+        }
+        __syncthreads();
+        for (int cc = 1 + threadIdx.x; cc <= kBandW; cc += blockDim.x) {
+            const int i = x0 - 1 + cc;
+            if (i < 0 || i > nx - 1) continue;  // the whole row, rim columns included
+#pragma unroll
+            for (int f = 0; f < NF; ++f) P.out[fidx[f]][cell(P, i, j)] = Fcur[f * CF + cc];
+        }
+        float* t = Fprev;
+        Fprev = Fcur;
+        Fcur = t;
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------- edge tiles
+template <int M, bool VEL>
+__device__ void edge_tile(const StepParams& P, const TiledArgs& T, int x0, int z0, int x_end, float* smem) {
+    using G = Geo<M>;
+    const int xa = x0 - kEdgeX, za = z0 - kEdgeZ;
+    float* sin = smem;
+    float* spre = smem + (VEL ? 3 : 2) * (G::RW + 2 * M) * (G::RH + 2 * M);
+    load_region_inputs<M, VEL>(P, xa, za, G::RW, G::RH, sin);
+    __syncthreads();
+    compute_region_pre<M, VEL>(P, T, xa, za, G::RW, G::RH, sin, spre);
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < kTX * kTZ; idx += blockDim.x) {
+        const int i = x0 + (idx % kTX), j = z0 + (idx / kTX);
+        if (i >= P.nx || i >= x_end || !row_stored(P, j)) continue;
+        const bool band = (i <= P.nbc) || (i >= P.nx - P.nbc - 1) || (!P.fs && j <= P.nbc);
+        const size_t c = cell(P, i, j);
+        if (VEL) {
+            float vx = SmemPre{spre, xa, za, G::RW, G::RH, 0}(i, j);
+            float vz = SmemPre{spre, xa, za, G::RW, G::RH, 1}(i, j);
+            if (band) {
+                vx = HabcPoint<SmemPre>{P, SmemPre{spre, xa, za, G::RW, G::RH, 0}, P.in[VX], P.w_tab[0]}.final_value(i, j);
+                vz = HabcPoint<SmemPre>{P, SmemPre{spre, xa, za, G::RW, G::RH, 1}, P.in[VZ], P.w_tab[1]}.final_value(i, j);
+            }
+            P.out[VX][c] = vx;
+            P.out[VZ][c] = vz;
+        } else {
+            float v[3];
+#pragma unroll
+            for (int f = 0; f < 3; ++f) {
+                const SmemPre pre{spre, xa, za, G::RW, G::RH, f};
+                v[f] = band ? HabcPoint<SmemPre>{P, pre, P.in[TXX + f], P.w_tab[2]}.final_value(i, j) : pre(i, j);
+            }
+            if (in_free_surface_rows(P, j)) v[1] = v[2] = 0.f;
+            P.out[TXX][c] = v[0];
+            P.out[TZZ][c] = v[1];
+            P.out[TXZ][c] = v[2];
+        }
+    }
+}
+
+// ---------------------------------------------------------------- fast tiles
+// x-derivative windows: NQ float4s starting HX cells left of the thread's
+// first column.  win[k] is the value at column x - HX + k.
+template <int M>
+__device__ __forceinline__ void load_xwin(const float* row, float (&win)[4 * Geo<M>::NQ]) {
+#pragma unroll
+    for (int q = 0; q < Geo<M>::NQ; ++q) {
+        const float4 v = lds4(row + 4 * q);
+        win[4 * q] = v.x;
+        win[4 * q + 1] = v.y;
+        win[4 * q + 2] = v.z;
+        win[4 * q + 3] = v.w;
+    }
+}
+
+// d[c] = sum_l a_l (win[HX+c+l-1+s] - win[HX+c-l+s]) for the thread's 4
+// columns: s = 0 for the "forward" staggering (f[i+l-1] - f[i-l]), s = 1 for
+// the "backward" one (f[i+l] - f[i-l+1]).
+template <int M, int S>
+__device__ __forceinline__ void xderiv(const StepParams& P, const float (&w)[4 * Geo<M>::NQ], float (&d)[4]) {
+    constexpr int HX = Geo<M>::HX;
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+        float acc = 0.f;
+#pragma unroll
+        for (int l = 1; l <= M; ++l) acc = fadd(fmul(P.a[l - 1], fsub(w[HX + c + l - 1 + S], w[HX + c - l + S])), acc);
+        d[c] = acc;
+    }
+}
+
+// z-derivatives of two rows from a (2M+1)-row window wz[0..2M] starting at
+// the window row of (row 0) - M + S: d[rr] = sum_l a_l (wz[rr+M+l-1] - wz[rr+M-l]),
+// evaluated as column pairs.
+template <int M>
+__device__ __forceinline__ void zderiv(const StepParams& P, const float4 (&wz)[2 * M + 1], float2 (&lo)[2],
+                                       float2 (&hi)[2]) {
+#pragma unroll
+    for (int rr = 0; rr < 2; ++rr) {
+        float2 a = make_float2(0.f, 0.f), b = make_float2(0.f, 0.f);
+#pragma unroll
+        for (int l = 1; l <= M; ++l) {
+            const float2 al = make_float2(P.a[l - 1], P.a[l - 1]);
+            a = add2(mul2(al, sub2(lo2(wz[rr + M + l - 1]), lo2(wz[rr + M - l]))), a);
+            b = add2(mul2(al, sub2(hi2(wz[rr + M + l - 1]), hi2(wz[rr + M - l]))), b);
+        }
+        lo[rr] = a;
+        hi[rr] = b;
+    }
+}
+
+// Stencil values of one tile cell, read back from shared memory by the HABC
+// rules of band tiles.
+struct TilePre {
+    const float* spre;
+    int x0, z0, f;
+    __device__ float operator()(int i, int j) const { return spre[(f * kTZ + (j - z0)) * kTX + (i - x0)]; }
+};
+
+template <int M>
+__device__ __forceinline__ void fast_vel(const StepParams& P, const TiledArgs& T, const VelMaps& mp, int x0, int z0,
+                                         int x_end, bool band, bool rim, float* smem) {
+    using G = Geo<M>;
+    constexpr int BOX = G::BOXS;
+    float* s_xx = smem;
+    float* s_zz = smem + BOX;
+    float* s_xz = smem + 2 * BOX;
+    float* p_vx = smem + 3 * BOX;
+    float* p_vz = p_vx + kPBox;
+    float* p_b0 = p_vz + kPBox;
+    float* p_b2 = p_b0 + kPBox;
+    float* p_b1 = T.iso ? p_b0 : p_b2 + kPBox;
+    float* p_b3 = T.iso ? p_b2 : p_b2 + 2 * kPBox;
+    uint64_t* bar = reinterpret_cast<uint64_t*>(p_b2 + (T.iso ? 1 : 3) * kPBox);
+    if (threadIdx.x == 0) {
+        mbar_init(bar, 1);
+        fence_barrier_init();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        mbar_expect_tx(bar, (3 * G::BOXW * G::BOXH + (T.iso ? 4 : 6) * kPBox) * 4);
+        tma_load_2d(s_xx, &mp.xx, x0 - G::HX, z0 - M, bar);
+        tma_load_2d(s_zz, &mp.zz, x0 - G::HX, z0 - M, bar);
+        tma_load_2d(s_xz, &mp.xz, x0 - G::HX, z0 - M, bar);
+        tma_load_2d(p_vx, &mp.vx, x0, z0, bar);
+        tma_load_2d(p_vz, &mp.vz, x0, z0, bar);
+        tma_load_2d(p_b0, &mp.b0, x0, z0, bar);
+        tma_load_2d(p_b2, &mp.b2, x0, z0, bar);
+        if (!T.iso) {
+            tma_load_2d(p_b1, &mp.b1, x0, z0, bar);
+            tma_load_2d(p_b3, &mp.b3, x0, z0, bar);
+        }
+    }
+    if (!wait_tma(bar, T)) return;
+    if (threadIdx.x == 0) {
+        const int si = P.src_i - (x0 - G::HX), sj = P.src_j - (z0 - M);
+        if (si >= 0 && si < G::BOXW && sj >= 0 && sj < G::BOXH) {
+            s_xx[sj * G::BOXW + si] = fadd(s_xx[sj * G::BOXW + si], P.src_w);
+            s_zz[sj * G::BOXW + si] = fadd(s_zz[sj * G::BOXW + si], P.src_w);
+        }
+    }
+    __syncthreads();
+
+    const int cg = threadIdx.x % kCG, rp = threadIdx.x / kCG;
+    const int x = x0 + 4 * cg, zt = z0 + 2 * rp;
+    const int xr = 4 * cg;  // box column of win[0] = column x - HX
+    float d1[2][4], d3[2][4];
+#pragma unroll
+    for (int rr = 0; rr < 2; ++rr) {
+        const int br = 2 * rp + rr + M;
+        float w[4 * G::NQ];
+        load_xwin<M>(s_xx + br * G::BOXW + xr, w);
+        xderiv<M, 0>(P, w, d1[rr]);  // dtxx/dx: txx[i+l-1] - txx[i-l]
+        load_xwin<M>(s_xz + br * G::BOXW + xr, w);
+        xderiv<M, 1>(P, w, d3[rr]);  // dtxz/dx: txz[i+l] - txz[i-l+1]
+    }
+    float2 d2lo[2], d2hi[2], d4lo[2], d4hi[2];
+    {
+        float4 wz[2 * M + 1];
+#pragma unroll
+        for (int k = 0; k <= 2 * M; ++k) wz[k] = lds4(s_xz + (2 * rp + k) * G::BOXW + xr + G::HX);
+        zderiv<M>(P, wz, d2lo, d2hi);  // dtxz/dz: txz[j+l-1] - txz[j-l]
+#pragma unroll
+        for (int k = 0; k <= 2 * M; ++k) wz[k] = lds4(s_zz + (2 * rp + 1 + k) * G::BOXW + xr + G::HX);
+        zderiv<M>(P, wz, d4lo, d4hi);  // dtzz/dz: tzz[j+l] - tzz[j-l+1]
+    }
+    float4 ox[2], oz[2];
+#pragma unroll
+    for (int rr = 0; rr < 2; ++rr) {
+        const int po = (2 * rp + rr) * kTX + xr;
+        const float4 vx = lds4(p_vx + po), vz = lds4(p_vz + po);
+        const float4 b0 = lds4(p_b0 + po), b1 = lds4(p_b1 + po), b2 = lds4(p_b2 + po), b3 = lds4(p_b3 + po);
+        const float2 xl = add2(lo2(vx), add2(mul2(lo2(b0), make_float2(d1[rr][0], d1[rr][1])), mul2(lo2(b1), d2lo[rr])));
+        const float2 xh = add2(hi2(vx), add2(mul2(hi2(b0), make_float2(d1[rr][2], d1[rr][3])), mul2(hi2(b1), d2hi[rr])));
+        const float2 zl = add2(lo2(vz), add2(mul2(lo2(b2), make_float2(d3[rr][0], d3[rr][1])), mul2(lo2(b3), d4lo[rr])));
+        const float2 zh = add2(hi2(vz), add2(mul2(hi2(b2), make_float2(d3[rr][2], d3[rr][3])), mul2(hi2(b3), d4hi[rr])));
+        ox[rr] = make_float4(xl.x, xl.y, xh.x, xh.y);
+        oz[rr] = make_float4(zl.x, zl.y, zh.x, zh.y);
+        if (rim) {  // cells outside the stencil domain keep their value
+#pragma unroll
+            for (int c = 0; c < 4; ++c)
+                if (!in_stencil(P, x + c, zt + rr)) {
+                    set_comp(ox[rr], c, comp(vx, c));
+                    set_comp(oz[rr], c, comp(vz, c));
+                }
+        }
+    }
+    if (band) {
+        __syncthreads();  // every thread is done with the boxes
+        float* spre = smem;  // [2][kTZ][kTX]
+#pragma unroll
+        for (int rr = 0; rr < 2; ++rr) {
+            const int po = (2 * rp + rr) * kTX + xr;
+            *reinterpret_cast<float4*>(spre + po) = ox[rr];
+            *reinterpret_cast<float4*>(spre + kPBox + po) = oz[rr];
+        }
+        __syncthreads();
+        const HabcPoint<TilePre> hx{P, TilePre{spre, x0, z0, 0}, P.in[VX], P.w_tab[0]};
+        const HabcPoint<TilePre> hz{P, TilePre{spre, x0, z0, 1}, P.in[VZ], P.w_tab[1]};
+#pragma unroll
+        for (int rr = 0; rr < 2; ++rr)
+#pragma unroll
+            for (int c = 0; c < 4; ++c)
+                if (x + c < x_end && row_stored(P, zt + rr) && lr_band_cell(P, x + c, zt + rr)) {
+                    set_comp(ox[rr], c, hx.final_value(x + c, zt + rr));
+                    set_comp(oz[rr], c, hz.final_value(x + c, zt + rr));
+                }
+    }
+    if (x < x_end) {
+#pragma unroll
+        for (int rr = 0; rr < 2; ++rr)
+            if (row_stored(P, zt + rr)) {
+                const size_t cc = cell(P, x, zt + rr);
+                stg4(P.out[VX] + cc, ox[rr]);
+                stg4(P.out[VZ] + cc, oz[rr]);
+            }
+    }
+}
+
+template <int M>
+__device__ __forceinline__ void fast_str(const StepParams& P, const TiledArgs& T, const StrMaps& mp, int x0, int z0,
+                                         int x_end, bool band, bool rim, float* smem) {
+    using G = Geo<M>;
+    constexpr int BOX = G::BOXS;
+    float* s_vx = smem;
+    float* s_vz = smem + BOX;
+    float* p_xx = smem + 2 * BOX;
+    float* p_zz = p_xx + kPBox;
+    float* p_xz = p_zz + kPBox;
+    float* p_lam = p_xz + kPBox;
+    float* p_mu = p_lam + kPBox;
+    float* p_mxz = p_mu + kPBox;
+    uint64_t* bar = reinterpret_cast<uint64_t*>(p_mxz + kPBox);
+    if (threadIdx.x == 0) {
+        mbar_init(bar, 1);
+        fence_barrier_init();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        mbar_expect_tx(bar, (2 * G::BOXW * G::BOXH + 6 * kPBox) * 4);
+        tma_load_2d(s_vx, &mp.vx, x0 - G::HX, z0 - M, bar);
+        tma_load_2d(s_vz, &mp.vz, x0 - G::HX, z0 - M, bar);
+        tma_load_2d(p_xx, &mp.txx, x0, z0, bar);
+        tma_load_2d(p_zz, &mp.tzz, x0, z0, bar);
+        tma_load_2d(p_xz, &mp.txz, x0, z0, bar);
+        tma_load_2d(p_lam, &mp.lam, x0, z0, bar);
+        tma_load_2d(p_mu, &mp.mu, x0, z0, bar);
+        tma_load_2d(p_mxz, &mp.mxz, x0, z0, bar);
+    }
+    if (!wait_tma(bar, T)) return;
+
+    const int cg = threadIdx.x % kCG, rp = threadIdx.x / kCG;
+    const int x = x0 + 4 * cg, zt = z0 + 2 * rp;
+    const int xr = 4 * cg;
+    float dxx[2][4], dzx[2][4];  // dvx/dx, dvz/dx
+#pragma unroll
+    for (int rr = 0; rr < 2; ++rr) {
+        const int br = 2 * rp + rr + M;
+        float w[4 * G::NQ];
+        load_xwin<M>(s_vx + br * G::BOXW + xr, w);
+        xderiv<M, 1>(P, w, dxx[rr]);  // vx[i+l] - vx[i-l+1]
+        load_xwin<M>(s_vz + br * G::BOXW + xr, w);
+        xderiv<M, 0>(P, w, dzx[rr]);  // vz[i+l-1] - vz[i-l]
+    }
+    float2 dzzlo[2], dzzhi[2], dxzlo[2], dxzhi[2];  // dvz/dz, dvx/dz
+    {
+        float4 wz[2 * M + 1];
+#pragma unroll
+        for (int k = 0; k <= 2 * M; ++k) wz[k] = lds4(s_vz + (2 * rp + k) * G::BOXW + xr + G::HX);
+        zderiv<M>(P, wz, dzzlo, dzzhi);  // vz[j+l-1] - vz[j-l]
+#pragma unroll
+        for (int k = 0; k <= 2 * M; ++k) wz[k] = lds4(s_vx + (2 * rp + 1 + k) * G::BOXW + xr + G::HX);
+        zderiv<M>(P, wz, dxzlo, dxzhi);  // vx[j+l] - vx[j-l+1]
+    }
+    float4 oxx[2], ozz[2], oxz[2];
+    const float2 dtx2 = make_float2(P.dtx, P.dtx), dtz2 = make_float2(P.dtz, P.dtz), two = make_float2(2.f, 2.f);
+#pragma unroll
+    for (int rr = 0; rr < 2; ++rr) {
+        const int po = (2 * rp + rr) * kTX + xr;
+        float4 txx = lds4(p_xx + po), tzz = lds4(p_zz + po);
+        const float4 txz = lds4(p_xz + po), lam = lds4(p_lam + po), mu = lds4(p_mu + po), mxz = lds4(p_mxz + po);
+        const int dc = P.src_i - x;
+        if (zt + rr == P.src_j && dc >= 0 && dc < 4) {
+            set_comp(txx, dc, fadd(comp(txx, dc), P.src_w));
+            set_comp(tzz, dc, fadd(comp(tzz, dc), P.src_w));
+        }
+        float2 r_xx[2], r_zz[2], r_xz[2];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const float2 lv = h ? hi2(lam) : lo2(lam), mv = h ? hi2(mu) : lo2(mu);
+            const float2 l2m = add2(lv, mul2(two, mv));
+            const float2 ex = mul2(make_float2(dxx[rr][2 * h], dxx[rr][2 * h + 1]), dtx2);
+            const float2 ez = mul2(h ? dzzhi[rr] : dzzlo[rr], dtz2);
+            r_xx[h] = add2(h ? hi2(txx) : lo2(txx), add2(mul2(l2m, ex), mul2(lv, ez)));
+            r_zz[h] = add2(h ? hi2(tzz) : lo2(tzz), add2(mul2(lv, ex), mul2(l2m, ez)));
+            const float2 sh = add2(mul2(h ? dxzhi[rr] : dxzlo[rr], dtz2),
+                                   mul2(make_float2(dzx[rr][2 * h], dzx[rr][2 * h + 1]), dtx2));
+            r_xz[h] = add2(h ? hi2(txz) : lo2(txz), mul2(h ? hi2(mxz) : lo2(mxz), sh));
+        }
+        oxx[rr] = make_float4(r_xx[0].x, r_xx[0].y, r_xx[1].x, r_xx[1].y);
+        ozz[rr] = make_float4(r_zz[0].x, r_zz[0].y, r_zz[1].x, r_zz[1].y);
+        oxz[rr] = make_float4(r_xz[0].x, r_xz[0].y, r_xz[1].x, r_xz[1].y);
+        if (rim) {
+#pragma unroll
+            for (int c = 0; c < 4; ++c)
+                if (!in_stencil(P, x + c, zt + rr)) {
+                    set_comp(oxx[rr], c, comp(txx, c));
+                    set_comp(ozz[rr], c, comp(tzz, c));
+                    set_comp(oxz[rr], c, comp(txz, c));
+                }
+        }
+    }
+    if (band) {
+        __syncthreads();
+        float* spre = smem;  // [3][kTZ][kTX]
+#pragma unroll
+        for (int rr = 0; rr < 2; ++rr) {
+            const int po = (2 * rp + rr) * kTX + xr;
+            *reinterpret_cast<float4*>(spre + po) = oxx[rr];
+            *reinterpret_cast<float4*>(spre + kPBox + po) = ozz[rr];
+            *reinterpret_cast<float4*>(spre + 2 * kPBox + po) = oxz[rr];
+        }
+        __syncthreads();
+        const HabcPoint<TilePre> h0{P, TilePre{spre, x0, z0, 0}, P.in[TXX], P.w_tab[2]};
+        const HabcPoint<TilePre> h1{P, TilePre{spre, x0, z0, 1}, P.in[TZZ], P.w_tab[2]};
+        const HabcPoint<TilePre> h2{P, TilePre{spre, x0, z0, 2}, P.in[TXZ], P.w_tab[2]};
+#pragma unroll
+        for (int rr = 0; rr < 2; ++rr)
+#pragma unroll
+            for (int c = 0; c < 4; ++c)
+                if (x + c < x_end && row_stored(P, zt + rr) && lr_band_cell(P, x + c, zt + rr)) {
+                    set_comp(oxx[rr], c, h0.final_value(x + c, zt + rr));
+                    set_comp(ozz[rr], c, h1.final_value(x + c, zt + rr));
+                    set_comp(oxz[rr], c, h2.final_value(x + c, zt + rr));
+                }
+    }
+    if (x < x_end) {
+#pragma unroll
+        for (int rr = 0; rr < 2; ++rr)
+            if (row_stored(P, zt + rr)) {
+                if (in_free_surface_rows(P, zt + rr)) {
+                    ozz[rr] = make_float4(0.f, 0.f, 0.f, 0.f);
+                    oxz[rr] = make_float4(0.f, 0.f, 0.f, 0.f);
+                }
+                const size_t cc = cell(P, x, zt + rr);
+                stg4(P.out[TXX] + cc, oxx[rr]);
+                stg4(P.out[TZZ] + cc, ozz[rr]);
+                stg4(P.out[TXZ] + cc, oxz[rr]);
+            }
+    }
+}
+
+// Block-uniform classification of a tile.
+struct TileKind {
+    bool generic, band, rim;
+    int x0, z0, x_end;
+};
+
+__device__ __forceinline__ TileKind classify(const StepParams& P, const TiledArgs& T, int tile) {
+    TileKind k;
+    const int tx = tile % T.tiles_x, tz = tile / T.tiles_x;
+    k.x0 = tile_x0(T, tx);
+    k.z0 = tz * kTZ;
+    // Stores stop at the previous column of the last tile, and never pass
+    // round_up(nx, 4) <= row pitch (grids narrower than one tile).
+    k.x_end = min((tx < T.tiles_x - 1) ? min(k.x0 + kTX, T.x_last) : k.x0 + kTX, (P.nx + 3) / 4 * 4);
+    const int b = P.nbc;
+    const bool band_cols = (k.x0 <= b) || (k.x0 + kTX - 1 >= P.nx - b - 1);
+    const int js0 = P.fs ? b : 1;
+    const bool lr_rows = (k.z0 + kTZ - 1 >= js0) && (k.z0 <= P.nz - b - 2);
+    k.band = band_cols && lr_rows;
+    const bool top = !P.fs && k.z0 <= b;
+    k.generic = top || (k.band && b + 6 > kTX);
+    k.rim = k.x0 < P.M || k.x0 + kTX > P.nx - P.M || k.z0 < P.M || k.z0 + kTZ > P.nz - P.M;
+    return k;
+}
+
+// ---------------------------------------------------------------- receivers
+__device__ inline void record_block(const StepParams& P, int rblock) {
+    const int r = rblock * blockDim.x + threadIdx.x;
+    if (r >= P.n_rec || P.rec_k < 1) return;
+    const int c = P.rec_cell[r];
+    float v;
+    if (P.rec_kind == 0) v = P.in[VZ][c];
+    else if (P.rec_kind == 1) v = P.in[VX][c];
+    else v = fmul(fadd(P.in[TXX][c], P.in[TZZ][c]), 0.5f);
+    P.gather[(size_t)(P.rec_k - 1) + (size_t)r * P.nt] = v;
+}
+
+// ---------------------------------------------------------------- kernels
+template <int M>
+__global__ void __launch_bounds__(kThreads, 5) velocity_kernel(const __grid_constant__ StepParams P, const __grid_constant__ TiledArgs T,
+                                                            const __grid_constant__ VelMaps maps) {
+    extern __shared__ __align__(128) float smem[];
+    int bid = blockIdx.x;
+    if (bid < T.n_band_blocks) {
+        band_block<M, true>(P, T, bid, smem);
+        return;
+    }
+    bid -= T.n_band_blocks;
+    if (bid < T.n_tile_blocks) {
+        const TileKind k = classify(P, T, bid);
+        if (k.generic) edge_tile<M, true>(P, T, k.x0, k.z0, k.x_end, smem);
+        else fast_vel<M>(P, T, maps, k.x0, k.z0, k.x_end, k.band, k.rim, smem);
+        return;
+    }
+    record_block(P, bid - T.n_tile_blocks);
+}
+
+template <int M>
+__global__ void __launch_bounds__(kThreads, 5) stress_kernel(const __grid_constant__ StepParams P, const __grid_constant__ TiledArgs T,
+                                                          const __grid_constant__ StrMaps maps) {
+    extern __shared__ __align__(128) float smem[];
+    int bid = blockIdx.x;
+    if (bid < T.n_band_blocks) {
+        band_block<M, false>(P, T, bid, smem);
+        return;
+    }
+    bid -= T.n_band_blocks;
+    if (bid < T.n_tile_blocks) {
+        const TileKind k = classify(P, T, bid);
+        if (k.generic) edge_tile<M, false>(P, T, k.x0, k.z0, k.x_end, smem);
+        else fast_str<M>(P, T, maps, k.x0, k.z0, k.x_end, k.band, k.rim, smem);
+    }
+}
+
+// Receivers of the last step (the velocity launch of step k records k-1).
+__global__ void record_kernel(const StepParams P) { record_block(P, blockIdx.x); }
+
+// Buoyancy dtx/rho_vx, dtz/rho_vx, dtx/rho_vz, dtz/rho_vz: the divisions of
+// update_velocity! (velocity.jl:41-42), IEEE-rounded, once per medium and dt.
+__global__ void buoyancy_kernel(const float* rho_vx, const float* rho_vz, float dtx, float dtz, size_t n,
+                                float* b0, float* b1, float* b2, float* b3) {
+    for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
+        const float rx = rho_vx[k], rz = rho_vz[k];
+        b0[k] = fdiv(dtx, rx);
+        b2[k] = fdiv(dtx, rz);
+        if (b1 != b0) b1[k] = fdiv(dtz, rx);
+        if (b3 != b2) b3[k] = fdiv(dtz, rz);
+    }
+}
+
+// Shared-memory bytes of one launch (the largest block role).
+template <int M>
+__host__ size_t tiled_smem_bytes(bool vel, int nbc, bool iso) {
+    using G = Geo<M>;
+    const int nin = vel ? 3 : 2, nout = vel ? 2 : 3;
+    const int npoint = vel ? (iso ? 4 : 6) : 6;
+    const size_t interior = ((size_t)nin * G::BOXS + (size_t)npoint * kPBox) * 4 + 16;
+    const size_t edge = ((size_t)nin * (G::RW + 2 * M) * (G::RH + 2 * M) + (size_t)nout * G::RW * G::RH) * 4;
+    const int C = kBandW + 6, R = nbc + 1;
+    const size_t band = (std::max((size_t)nin * (C + 2 * M) * (R + 2 * M), (size_t)nout * R * C) +
+                         (size_t)nout * R * C + 2 * (size_t)nout * (kBandW + 2)) * 4;
+    return std::max(interior, std::max(edge, band));
+}
+
+}  // namespace fomo

@@ -85,6 +85,11 @@ CASES = [
     layered(50, 22, seed=8, nbc=17, fd_order=8, nt=90, water_rows=2),
     _band_source_case(),
     _right_band_source_case(),
+    # grids several tiles wide: interior tiles, a right-aligned last tile, nx % 4 != 0
+    layered(231, 90, seed=13, nbc=10, fd_order=8, nt=100, n_rec=41),
+    layered(205, 75, seed=14, nbc=12, fd_order=12, nt=90, free_surface=False, rec_type="p"),
+    layered(150, 70, seed=15, nbc=60, fd_order=4, nt=80, rec_type="vx"),   # band wider than a fast tile allows
+    layered(190, 96, seed=16, nbc=20, fd_order=6, nt=90, water_rows=6, n_rec=23),
 ]
 
 

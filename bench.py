@@ -327,9 +327,12 @@ def b200_arm(args, rank, world, local):
     roofline = None
     if dom:
         traffic = None
-        tf = os.path.join(REPO, "profiles", "traffic.json")
+        tf = os.path.join(REPO, "profiles", "dram_traffic_per_launch.txt")
         if os.path.exists(tf):
-            traffic = json.load(open(tf)).get(dom["name"])
+            for line in open(tf):
+                f = line.split()
+                if len(f) >= 2 and not line.startswith("#") and f[0] == dom["name"]:
+                    traffic = float(f[1])
         roofline = {"bound": "hbm", "kernel": dom["name"], "achieved": dom["gbs"], "peak": peak, "unit": "GB/s",
                     "frac": dom["gbs"] / peak, "peak_source": f"{peak_src} (MEASURED_PEAKS.json hbm_gbs)",
                     "traffic": traffic,

@@ -821,3 +821,252 @@ int fomo_b200_run_shot(uint64_t medium, uint64_t wavefield, const FomoHabc* habc
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Allocation-free shot: fomo_b200_run_shot_noalloc.
+//
+// Some callers cannot call cudaMalloc while they run a shot: a caller that is
+// capturing its stream into a CUDA graph (allocation is not a capturable
+// operation), a serving loop whose memory is carved once from a fixed pool at
+// start-up, or a host framework that forbids device allocation (and the
+// device-wide synchronisation cudaFree implies) on its latency path.  For them
+// this entry point runs the same time-step kernels with every scratch buffer
+// taken from one static device array: the two wavefield copies, the buoyancy
+// arrays, the HABC weight tables, the receiver offsets and the kernels' status
+// word.  The caller passes the inputs (medium, on the device) and the output
+// (gather, on the device); nothing is allocated or freed.
+//
+// The array (kNoAllocScratchBytes) is part of the library's device image, so
+// every GPU that loads the library holds it until the process exits.  All
+// calls share it and it keeps the last call's contents: each call clears the
+// wavefield and the status word before its first step.  Calls that overlap on
+// the GPU (two streams, two threads, two devices' worth of work aimed at one
+// device) race on the array; callers must serialise them.
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr size_t kNoAllocScratchBytes = 48ull << 20;  // 48 MiB
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mu;
+unsigned char* g_noalloc_ptr[kMaxDevices] = {nullptr};
+
+inline size_t align256(size_t n) { return (n + 255) / 256 * 256; }
+
+// Device address of the scratch array for the current device.  The first call
+// on a device resolves it (cudaGetSymbolAddress, with that device current).
+int noalloc_scratch(unsigned char** out) {
+    int dev = -1;
+    CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kMaxDevices) return fail(FOMO_EINVAL, "device ordinal %d out of range", dev);
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_ptr[dev]) {
+        void* p = nullptr;
+        CUDA_TRY(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+        g_noalloc_ptr[dev] = static_cast<unsigned char*>(p);
+    }
+    *out = g_noalloc_ptr[dev];
+    return FOMO_OK;
+}
+
+template <int M>
+int noalloc_loop(const fomo::StepParams& P0, fomo::TiledArgs T, float* fields, int pitch, int nx, int nz,
+                 const float* const* med, const float* const* buoy, const float* wavelet, int n_wavelet,
+                 int nt, int n_rec, cudaStream_t st) {
+    using G = fomo::Geo<M>;
+    const bool iso = T.iso != 0;
+    const size_t plane = (size_t)pitch * nz;
+    auto field = [&](int copy, int q) { return fields + ((size_t)copy * 5 + q) * plane; };
+    CUtensorMap halo[2][5], tile[2][5], mod[3], bm[4];
+    for (int c = 0; c < 2; ++c)
+        for (int q = 0; q < 5; ++q) {
+            if (int rc = encode_map(&halo[c][q], field(c, q), nx, nz, pitch, G::BOXW, G::BOXH)) return rc;
+            if (int rc = encode_map(&tile[c][q], field(c, q), nx, nz, pitch, fomo::kTX, fomo::kTZ)) return rc;
+        }
+    for (int q = 0; q < 3; ++q)
+        if (int rc = encode_map(&mod[q], med[2 + q], nx, nz, pitch, fomo::kTX, fomo::kTZ)) return rc;
+    for (int q = 0; q < 4; ++q)
+        if (int rc = encode_map(&bm[q], buoy[q], nx, nz, pitch, fomo::kTX, fomo::kTZ)) return rc;
+    const Launch L = launch_shape<M>(nx, nz, P0.nbc, iso);
+    if (L.smem_v > 48 * 1024)
+        CUDA_TRY(cudaFuncSetAttribute(fomo::velocity_kernel<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.smem_v));
+    if (L.smem_s > 48 * 1024)
+        CUDA_TRY(cudaFuncSetAttribute(fomo::stress_kernel<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.smem_s));
+    T.n_band_blocks = L.n_band;
+    T.n_tile_blocks = L.n_tile;
+    T.tiles_x = L.tiles_x;
+    T.x_last = L.x_last;
+    const int rec_blocks = (n_rec + fomo::kThreads - 1) / fomo::kThreads;
+    int cur = 0;
+    for (int k = 1; k <= nt; ++k) {
+        const int a = cur, b = 1 - cur;
+        fomo::StepParams P = P0;
+        P.src_w = (k <= n_wavelet) ? wavelet[k - 1] : 0.f;
+        for (int q = 0; q < 5; ++q) P.in[q] = field(a, q);
+        P.out[fomo::VX] = field(b, fomo::VX);
+        P.out[fomo::VZ] = field(b, fomo::VZ);
+        P.rec_k = (k >= 2 && n_rec > 0) ? k - 1 : 0;
+        fomo::VelMaps vm;
+        vm.xx = halo[a][fomo::TXX];
+        vm.zz = halo[a][fomo::TZZ];
+        vm.xz = halo[a][fomo::TXZ];
+        vm.vx = tile[a][fomo::VX];
+        vm.vz = tile[a][fomo::VZ];
+        vm.b0 = bm[0];
+        vm.b1 = bm[1];
+        vm.b2 = bm[2];
+        vm.b3 = bm[3];
+        fomo::velocity_kernel<M><<<L.n_band + L.n_tile + (P.rec_k ? rec_blocks : 0), fomo::kThreads, L.smem_v, st>>>(P, T, vm);
+        P.in[fomo::VX] = field(b, fomo::VX);
+        P.in[fomo::VZ] = field(b, fomo::VZ);
+        for (int q = 2; q < 5; ++q) P.out[q] = field(b, q);
+        P.out[fomo::VX] = P.out[fomo::VZ] = nullptr;
+        P.rec_k = 0;
+        fomo::StrMaps sm;
+        sm.vx = halo[b][fomo::VX];
+        sm.vz = halo[b][fomo::VZ];
+        sm.txx = tile[a][fomo::TXX];
+        sm.tzz = tile[a][fomo::TZZ];
+        sm.txz = tile[a][fomo::TXZ];
+        sm.lam = mod[0];
+        sm.mu = mod[1];
+        sm.mxz = mod[2];
+        fomo::stress_kernel<M><<<L.n_band + L.n_tile, fomo::kThreads, L.smem_s, st>>>(P, T, sm);
+        cur = b;
+    }
+    if (n_rec > 0 && nt > 0) {  // receivers of the last step
+        fomo::StepParams P = P0;
+        for (int q = 0; q < 5; ++q) P.in[q] = field(cur, q);
+        P.rec_k = nt;
+        fomo::record_kernel<<<rec_blocks, fomo::kThreads, 0, st>>>(P);
+    }
+    CUDA_TRY(cudaGetLastError());
+    return FOMO_OK;
+}
+
+}  // namespace
+
+extern "C" int fomo_b200_run_shot_noalloc(int32_t nx, int32_t nz, int32_t M, int32_t pad, int32_t free_surface,
+                                          const float* rho_vx, const float* rho_vz, const float* lam,
+                                          const float* mu_txx, const float* mu_txz, int32_t pitch,
+                                          const FomoHabc* habc, const FomoShot* shot, float* gather_out,
+                                          void* stream) {
+    if (!rho_vx || !rho_vz || !lam || !mu_txx || !mu_txz || !habc || !shot)
+        return fail(FOMO_EINVAL, "NULL argument");
+    if (int rc = check_medium_args(nx, nz, M, pad)) return rc;
+    if (free_surface && pad < 5) return fail(FOMO_EINVAL, "free surface needs pad >= 5 (rows pad-4..pad+1), got %d", pad);
+    if (pitch < (nx + 3) / 4 * 4 || pitch % 4)
+        return fail(FOMO_EINVAL, "row pitch %d must be a multiple of 4 floats and >= round_up(nx, 4) = %d", pitch,
+                    (nx + 3) / 4 * 4);
+    const float* med[5] = {rho_vx, rho_vz, lam, mu_txx, mu_txz};
+    for (int q = 0; q < 5; ++q)
+        if ((uintptr_t)med[q] % 16) return fail(FOMO_EINVAL, "medium array %d is not 16-byte aligned", q);
+    if (shot->M != M || !shot->a) return fail(FOMO_EINVAL, "shot M=%d differs from medium M=%d or no coefficients", shot->M, M);
+    if (shot->nt < 0 || shot->n_wavelet < 0 || (shot->n_wavelet > 0 && !shot->wavelet)) return fail(FOMO_EINVAL, "bad nt or wavelet");
+    const int nbc = habc->nbc;
+    if (nbc < 1 || 2 * nbc + 3 > nx || 2 * nbc + 2 > nz) return fail(FOMO_EINVAL, "nbc=%d does not fit the %dx%d grid", nbc, nx, nz);
+    if (!habc->w_vx || !habc->w_vz || !habc->w_tau) return fail(FOMO_EINVAL, "HABC weight tables are NULL");
+    if (shot->src_i < 1 || shot->src_i > nx || shot->src_j < 1 || shot->src_j > nz)
+        return fail(FOMO_EINVAL, "source (%d, %d) outside the %dx%d grid", shot->src_i, shot->src_j, nx, nz);
+    if (shot->rec_kind < 0 || shot->rec_kind > 2) return fail(FOMO_EINVAL, "bad receiver kind %d", shot->rec_kind);
+    if (shot->n_rec < 0 || (shot->n_rec > 0 && (!shot->rec_i || !shot->rec_j || !gather_out)))
+        return fail(FOMO_EINVAL, "bad receiver arrays or gather pointer");
+    std::vector<int> cells(shot->n_rec);
+    for (int r = 0; r < shot->n_rec; ++r) {
+        const int i = shot->rec_i[r], j = shot->rec_j[r];
+        if (i < 1 || i > nx || j < 1 || j > nz)
+            return fail(FOMO_EINVAL, "receiver %d at (%d, %d) outside the %dx%d grid", r + 1, i, j, nx, nz);
+        cells[r] = (i - 1) + (j - 1) * pitch;
+    }
+    // Carve the scratch: status | tables | receiver offsets | buoyancy | wavefield.
+    const bool iso = shot->dtx == shot->dtz;
+    const size_t plane = (size_t)pitch * nz * sizeof(float);
+    const size_t off_tab = 256;
+    const size_t off_rec = off_tab + align256(3 * (size_t)(nbc + 2) * sizeof(float));
+    const size_t off_buo = off_rec + align256((size_t)shot->n_rec * sizeof(int));
+    const size_t off_wf = off_buo + align256((iso ? 2 : 4) * plane);
+    const size_t need = off_wf + 10 * plane;
+    if (need > kNoAllocScratchBytes)
+        return fail(FOMO_EINVAL, "shot needs %zu bytes of scratch, more than the %zu-byte static array of "
+                    "fomo_b200_run_shot_noalloc (grid %dx%d, pitch %d, %d receivers)", need, kNoAllocScratchBytes,
+                    nx, nz, pitch, shot->n_rec);
+    unsigned char* base = nullptr;
+    if (int rc = noalloc_scratch(&base)) return rc;
+    cudaStream_t st = (cudaStream_t)stream;
+    int* d_status = reinterpret_cast<int*>(base);
+    float* d_tabs = reinterpret_cast<float*>(base + off_tab);
+    int* d_rec = reinterpret_cast<int*>(base + off_rec);
+    float* d_buo = reinterpret_cast<float*>(base + off_buo);
+    float* d_fields = reinterpret_cast<float*>(base + off_wf);
+    const size_t tab_n = (size_t)nbc + 2;
+    CUDA_TRY(cudaMemsetAsync(d_status, 0, sizeof(int), st));
+    CUDA_TRY(cudaMemsetAsync(d_fields, 0, 10 * plane, st));
+    CUDA_TRY(cudaMemcpyAsync(d_tabs, habc->w_vx, tab_n * 4, cudaMemcpyHostToDevice, st));
+    CUDA_TRY(cudaMemcpyAsync(d_tabs + tab_n, habc->w_vz, tab_n * 4, cudaMemcpyHostToDevice, st));
+    CUDA_TRY(cudaMemcpyAsync(d_tabs + 2 * tab_n, habc->w_tau, tab_n * 4, cudaMemcpyHostToDevice, st));
+    if (shot->n_rec) CUDA_TRY(cudaMemcpyAsync(d_rec, cells.data(), cells.size() * sizeof(int), cudaMemcpyHostToDevice, st));
+    const size_t pf = (size_t)pitch * nz;
+    float* b0 = d_buo;
+    float* b2 = d_buo + pf;
+    float* b1 = iso ? b0 : d_buo + 2 * pf;
+    float* b3 = iso ? b2 : d_buo + 3 * pf;
+    fomo::buoyancy_kernel<<<4 * 148, 256, 0, st>>>(rho_vx, rho_vz, shot->dtx, shot->dtz, pf, b0, b1, b2, b3);
+    CUDA_TRY(cudaGetLastError());
+
+    fomo::StepParams P;
+    std::memset(&P, 0, sizeof(P));
+    P.nx = nx;
+    P.nz = nz;
+    P.pitch = pitch;
+    P.M = M;
+    P.pad = pad;
+    P.nbc = nbc;
+    P.fs = free_surface ? 1 : 0;
+    P.dtx = shot->dtx;
+    P.dtz = shot->dtz;
+    for (int l = 0; l < M; ++l) P.a[l] = shot->a[l];
+    P.qx = habc->qx;
+    P.qz = habc->qz;
+    P.qt_x = habc->qt_x;
+    P.qt_z = habc->qt_z;
+    P.qxt = habc->qxt;
+    for (int t = 0; t < 3; ++t) P.w_tab[t] = d_tabs + t * tab_n;
+    P.rho_vx = rho_vx;
+    P.rho_vz = rho_vz;
+    P.lam = lam;
+    P.mu_txx = mu_txx;
+    P.mu_txz = mu_txz;
+    P.src_i = shot->src_i - 1;
+    P.src_j = shot->src_j - 1;
+    P.nt = shot->nt;
+    P.n_rec = shot->n_rec;
+    P.rec_kind = shot->rec_kind;
+    P.rec_cell = d_rec;
+    P.gather = gather_out;
+    fomo::TiledArgs T;
+    std::memset(&T, 0, sizeof(T));
+    T.b[0] = b0;
+    T.b[1] = b1;
+    T.b[2] = b2;
+    T.b[3] = b3;
+    T.iso = iso ? 1 : 0;
+    T.status = d_status;
+    const float* bp[4] = {b0, b1, b2, b3};
+    int rc = FOMO_EINVAL;
+    switch (M) {
+        case 1: rc = noalloc_loop<1>(P, T, d_fields, pitch, nx, nz, med, bp, shot->wavelet, shot->n_wavelet, shot->nt, shot->n_rec, st); break;
+        case 2: rc = noalloc_loop<2>(P, T, d_fields, pitch, nx, nz, med, bp, shot->wavelet, shot->n_wavelet, shot->nt, shot->n_rec, st); break;
+        case 3: rc = noalloc_loop<3>(P, T, d_fields, pitch, nx, nz, med, bp, shot->wavelet, shot->n_wavelet, shot->nt, shot->n_rec, st); break;
+        case 4: rc = noalloc_loop<4>(P, T, d_fields, pitch, nx, nz, med, bp, shot->wavelet, shot->n_wavelet, shot->nt, shot->n_rec, st); break;
+        case 5: rc = noalloc_loop<5>(P, T, d_fields, pitch, nx, nz, med, bp, shot->wavelet, shot->n_wavelet, shot->nt, shot->n_rec, st); break;
+        case 6: rc = noalloc_loop<6>(P, T, d_fields, pitch, nx, nz, med, bp, shot->wavelet, shot->n_wavelet, shot->nt, shot->n_rec, st); break;
+    }
+    if (rc) return rc;
+    int status = 0;
+    CUDA_TRY(cudaMemcpyAsync(&status, d_status, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    if (status == fomo::kErrTmaTimeout) return fail(FOMO_ETIMEOUT, "a TMA load of a time-step kernel did not complete");
+    if (status) return fail(FOMO_ECUDA, "time-step kernel reported error %d", status);
+    return FOMO_OK;
+}

@@ -201,6 +201,44 @@ typedef struct {
 int fomo_b200_shot_profile(uint64_t shot_handle, int32_t n_steps, FomoKernelTime* out,
                            int32_t max_kinds, int32_t* n_kinds);
 
+/* Allocation-free shot.  No counterpart in the reference: it exists for
+ * callers that cannot allocate device memory while a shot runs -- a caller
+ * capturing its stream into a CUDA graph (allocation cannot be captured), a
+ * serving loop that carves all memory from a fixed pool at start-up, or a
+ * host framework that forbids cudaMalloc/cudaFree (and the device-wide
+ * synchronisation cudaFree implies) on its latency path.
+ *
+ * Runs the same kernels as fomo_b200_run_shot and calls no cudaMalloc,
+ * cudaFree or allocating library routine.  Every scratch buffer (both
+ * wavefield copies, the buoyancy arrays, HABC tables, receiver offsets, the
+ * kernels' status word) comes from one static device array of 48 MiB that
+ * every GPU loading the library holds until the process exits; grids whose
+ * scratch does not fit are rejected with FOMO_EINVAL and a message giving
+ * the bytes needed.  The scratch is 10 fields (+2 buoyancy arrays when
+ * dtx == dtz, +4 otherwise) of pitch*nz floats plus a few KB, so for example a
+ * 1000 x 1000 padded grid with dtx == dtz fits.
+ *
+ * Inputs: the five medium arrays on the device (each pitch*nz floats, row
+ * pitch `pitch` floats: a multiple of 4 and >= round_up(nx, 4); 16-byte
+ * aligned), the HABC and shot descriptions as for fomo_b200_run_shot (host
+ * structs).  Output: gather_out, a device array of nt*n_rec floats
+ * ([nt x n_rec] column major).  Work is queued on `stream` (a cudaStream_t,
+ * NULL for the legacy default stream) and the call returns once it is done.
+ * fomo_b200_init is not required; the current CUDA device is used.
+ *
+ * The first call on a device resolves the array's device address
+ * (cudaGetSymbolAddress), so make that first call before any stream capture.
+ * All calls share the array and it keeps the last call's contents; each call
+ * clears what must start at zero.  Calls that overlap on the GPU race on the
+ * array: serialise them. */
+int fomo_b200_run_shot_noalloc(int32_t nx, int32_t nz, int32_t M, int32_t pad,
+                               int32_t free_surface, const float* rho_vx,
+                               const float* rho_vz, const float* lam,
+                               const float* mu_txx, const float* mu_txz,
+                               int32_t pitch, const FomoHabc* habc,
+                               const FomoShot* shot, float* gather_out,
+                               void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -60,6 +60,25 @@ class FomoKernelTime(ctypes.Structure):
                 ("bytes_per_launch", ctypes.c_double)]
 
 
+class FomoServerConfig(ctypes.Structure):
+    _fields_ = [("hbm_budget_bytes", ctypes.c_uint64), ("max_shots", ctypes.c_int32),
+                ("steps_per_launch", ctypes.c_int32)]
+
+
+class FomoRequestStats(ctypes.Structure):
+    _fields_ = [("queue_ms", ctypes.c_double), ("run_ms", ctypes.c_double), ("latency_ms", ctypes.c_double),
+                ("steps", ctypes.c_int32), ("batch_peak", ctypes.c_int32)]
+
+
+class FomoServerStats(ctypes.Structure):
+    _fields_ = [("submitted", ctypes.c_int64), ("completed", ctypes.c_int64), ("failed", ctypes.c_int64),
+                ("cancelled", ctypes.c_int64), ("batch_steps", ctypes.c_int64),
+                ("kernel_launches", ctypes.c_int64), ("graph_replays", ctypes.c_int64),
+                ("h2d_bytes", ctypes.c_int64), ("d2h_bytes", ctypes.c_int64),
+                ("peak_shots", ctypes.c_int32), ("steps_per_launch", ctypes.c_int32),
+                ("peak_bytes", ctypes.c_uint64)]
+
+
 # Every symbol include/fomo_b200.h declares, with its ctypes signature.
 _U64 = ctypes.c_uint64
 _P = ctypes.c_void_p
@@ -93,6 +112,16 @@ SIGNATURES = {
     "fomo_b200_shot_profile": [_U64, _I32, ctypes.POINTER(FomoKernelTime), _I32, ctypes.POINTER(_I32)],
     "fomo_b200_run_shot_noalloc": [_I32, _I32, _I32, _I32, _I32, _P, _P, _P, _P, _P, _I32,
                                    ctypes.POINTER(FomoHabc), ctypes.POINTER(FomoShot), _P, _P],
+    "fomo_b200_run_batch": [_U64, ctypes.POINTER(FomoHabc), ctypes.POINTER(FomoShot), _I32,
+                            ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(FomoRunStats)],
+    "fomo_b200_server_create": [ctypes.POINTER(FomoServerConfig), ctypes.POINTER(_U64)],
+    "fomo_b200_server_submit": [_U64, _U64, ctypes.POINTER(FomoHabc), ctypes.POINTER(FomoShot), _P,
+                                ctypes.POINTER(_U64)],
+    "fomo_b200_server_poll": [_U64, _U64, ctypes.POINTER(_I32)],
+    "fomo_b200_server_wait": [_U64, _U64, ctypes.c_double, ctypes.POINTER(FomoRequestStats)],
+    "fomo_b200_server_cancel": [_U64, _U64],
+    "fomo_b200_server_stats": [_U64, ctypes.POINTER(FomoServerStats)],
+    "fomo_b200_server_destroy": [_U64],
 }
 
 _lib = None

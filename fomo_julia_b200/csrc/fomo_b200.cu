@@ -8,6 +8,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -68,6 +69,7 @@ struct Medium : Object {
     bool maps_ok = false;
     CUtensorMap mod_maps[3];   // tile boxes of lam, mu_txx, mu_txz
     CUtensorMap buoy_maps[4];  // tile boxes of the four buoyancy arrays
+    std::atomic<int> users{0}; // shot-server requests holding this medium
     const float* arr(int q) const { return base + (size_t)q * pitch * nz; }
     ~Medium() override {
         if (base) cudaFree(base);
@@ -246,7 +248,7 @@ Launch launch_shape(int nx, int nz, int nbc, bool iso) {
     L.tiles_z = (nz + fomo::kTZ - 1) / fomo::kTZ;
     L.x_last = std::max(0, (nx + 3) / 4 * 4 - fomo::kTX);  // last tile ends at the grid's right edge
     L.n_tile = L.tiles_x * L.tiles_z;
-    L.n_band = (nx + fomo::kBandW - 1) / fomo::kBandW;
+    L.n_band = fomo::band_block_count(nx);
     L.smem_v = fomo::tiled_smem_bytes<M>(true, nbc, iso);
     L.smem_s = fomo::tiled_smem_bytes<M>(false, nbc, iso);
     return L;
@@ -412,6 +414,8 @@ int run_steps(Shot& s, int n_steps, Profile* prof = nullptr) {
 }
 
 // Records the receivers of the last step done (the next velocity launch would).
+void shutdown_servers();  // server.cuh
+
 int record_last(Shot& s) {
     auto& C = ctx();
     if (s.n_rec == 0 || s.k_done < 1 || s.recorded >= s.k_done) return FOMO_OK;
@@ -462,6 +466,7 @@ int fomo_b200_init(int device) {
 }
 
 int fomo_b200_shutdown(void) {
+    shutdown_servers();
     auto& C = ctx();
     std::lock_guard<std::mutex> lk(C.mu);
     if (!C.inited) return FOMO_OK;
@@ -588,7 +593,10 @@ int fomo_b200_medium_create(int32_t nx, int32_t nz, int32_t M, int32_t pad, int3
 int fomo_b200_medium_destroy(uint64_t medium) {
     std::lock_guard<std::mutex> lk(ctx().mu);
     if (int rc = ensure_init()) return rc;
-    if (!get<Medium>(medium)) return fail(FOMO_EINVAL, "unknown medium handle %llu", (unsigned long long)medium);
+    Medium* m = get<Medium>(medium);
+    if (!m) return fail(FOMO_EINVAL, "unknown medium handle %llu", (unsigned long long)medium);
+    if (int n = m->users.load())
+        return fail(FOMO_EINVAL, "medium %llu is in use by %d shot-server request(s)", (unsigned long long)medium, n);
     cudaStreamSynchronize(ctx().stream);
     ctx().objs.erase(medium);
     return FOMO_OK;
@@ -1070,3 +1078,5 @@ extern "C" int fomo_b200_run_shot_noalloc(int32_t nx, int32_t nz, int32_t M, int
     if (status) return fail(FOMO_ECUDA, "time-step kernel reported error %d", status);
     return FOMO_OK;
 }
+
+#include "server.cuh"

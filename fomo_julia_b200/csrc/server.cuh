@@ -1,0 +1,1347 @@
+// server.cuh -- the shot server (continuous batching) and fomo_b200_run_batch.
+//
+// Part of fomo_b200.cu's translation unit (included after the runtime's
+// internals: fail, ctx, Medium, encode_map, Launch, ...).
+//
+// One worker thread per server owns a CUDA stream, a stream-ordered memory
+// pool and the batch loop:
+//   admit   queued requests, in arrival order, while their device bytes fit
+//           the HBM budget (and the shot limit); allocate and upload each
+//           shot, starting it at the next batch step;
+//   run     K batch steps: per FD order, one velocity and one stress launch
+//           over every shot in flight (step_batch.cuh), then the step-counter
+//           advance; K steps are one CUDA graph replay once captured;
+//   retire  shots whose nt steps are done: record the last step's receivers,
+//           copy the gather to pinned memory, free the shot's memory (stream
+//           ordered), and hand the gather to the caller once its copy lands.
+// The host never waits for the GPU to decide what to run: shot lifetimes are
+// known in steps, so chunks are planned ahead and at most two are in flight.
+#pragma once
+
+#include <chrono>
+#include <condition_variable>
+#include <deque>
+#include <map>
+#include <thread>
+#include <tuple>
+
+#include "step_batch.cuh"
+
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+double ms_between(Clock::time_point a, Clock::time_point b) {
+    return std::chrono::duration<double, std::milli>(b - a).count();
+}
+
+inline size_t align_up(size_t n, size_t a) { return (n + a - 1) / a * a; }
+
+// Pinned host buffers, reused by size.
+class PinnedPool {
+  public:
+    ~PinnedPool() {
+        for (auto& b : size_) cudaFreeHost(b.first);
+    }
+    void* take(size_t n) {
+        n = std::max<size_t>(align_up(n, 4096), 4096);
+        auto it = free_.lower_bound(n);
+        if (it != free_.end() && it->first <= 4 * n) {
+            void* p = it->second;
+            free_.erase(it);
+            return p;
+        }
+        void* p = nullptr;
+        if (cudaHostAlloc(&p, n, cudaHostAllocDefault) != cudaSuccess) return nullptr;
+        size_[p] = n;
+        return p;
+    }
+    void give(void* p) {
+        if (p) free_.emplace(size_[p], p);
+    }
+
+  private:
+    std::multimap<size_t, void*> free_;
+    std::unordered_map<void*, size_t> size_;
+};
+
+enum ReqState { kQueued = 0, kRunning = 1, kDone = 2, kFailed = 3, kCancelled = 4 };
+
+// Buoyancy and descriptors of a medium for one (dtx, dtz), shared by the
+// server's shots on it.
+struct Resident {
+    Medium* med = nullptr;
+    float dtx = 0, dtz = 0;
+    int iso = 0;
+    float* buoy = nullptr;
+    const float* b[4] = {nullptr, nullptr, nullptr, nullptr};
+    CUtensorMap bmap[4];
+    CUtensorMap mod[3];
+    int refs = 0;
+    size_t bytes = 0;
+};
+
+struct Request {
+    uint64_t ticket = 0;
+    Medium* med = nullptr;
+    int M = 0, nbc = 0, nt = 0, src_i = 0, src_j = 0, n_rec = 0, rec_kind = 0;
+    float q[5] = {0, 0, 0, 0, 0};
+    float a[fomo::kMaxM] = {0};
+    float dtx = 0, dtz = 0;
+    std::vector<float> tabs, wavelet;
+    std::vector<int> cells;
+    float* gather_out = nullptr;
+    size_t bytes = 0;        // device bytes of the shot itself
+    size_t buoy_bytes = 0;   // device bytes of its medium's buoyancy
+    // Guarded by Server::mu_.
+    int state = kQueued, rc = FOMO_OK;
+    std::string err;
+    Clock::time_point t_submit, t_admit, t_done;
+    int batch_peak = 0;
+    // Worker only.
+    unsigned char* d_block = nullptr;
+    float* d_gather = nullptr;
+    Resident* res = nullptr;
+    int start = 0;           // batch step of the shot's step 1
+    size_t tabs_off = 0, cells_off = 0, wav_off = 0, gather_off = 0;
+    fomo::ShotDev dev;       // host image of the shot's table entry
+    void* staging = nullptr; // pinned: gather + status word
+    cudaEvent_t done_ev = nullptr;
+};
+
+// K candidates of the autotuner: 1 = plain launches (chunks of kPlainChunk
+// steps), otherwise one graph of K steps.
+constexpr int kTuneK[3] = {1, 8, 32};
+constexpr int kPlainChunk = 32;
+
+struct TuneKey {
+    int nx, nz, M, shots_log2;
+    bool operator<(const TuneKey& o) const {
+        return std::tie(nx, nz, M, shots_log2) < std::tie(o.nx, o.nz, o.M, o.shots_log2);
+    }
+};
+struct TuneEntry {
+    double ms_per_step[3] = {-1, -1, -1};
+    int chosen = -1;
+};
+std::mutex g_tune_mu;
+std::map<TuneKey, TuneEntry> g_tune;  // process-wide cache: (grid, order, batch size) -> K
+
+// Largest dynamic shared memory set so far for the batch kernels, per M.
+std::mutex g_batch_attr_mu;
+size_t g_batch_smem[2][fomo::kMaxM + 1] = {};
+
+size_t batch_smem_any(int M, bool vel, int nbc, bool iso) {
+    switch (M) {
+        case 1: return fomo::tiled_smem_bytes<1>(vel, nbc, iso);
+        case 2: return fomo::tiled_smem_bytes<2>(vel, nbc, iso);
+        case 3: return fomo::tiled_smem_bytes<3>(vel, nbc, iso);
+        case 4: return fomo::tiled_smem_bytes<4>(vel, nbc, iso);
+        case 5: return fomo::tiled_smem_bytes<5>(vel, nbc, iso);
+        case 6: return fomo::tiled_smem_bytes<6>(vel, nbc, iso);
+    }
+    return 0;
+}
+
+template <int M>
+int set_batch_smem_M(size_t v, size_t s) {
+    std::lock_guard<std::mutex> lk(g_batch_attr_mu);
+    if (v > g_batch_smem[0][M] && v + fomo::kBatchStaticSmem > 48 * 1024) {
+        CUDA_TRY(cudaFuncSetAttribute(fomo::batch_velocity_kernel<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)v));
+        g_batch_smem[0][M] = v;
+    }
+    if (s > g_batch_smem[1][M] && s + fomo::kBatchStaticSmem > 48 * 1024) {
+        CUDA_TRY(cudaFuncSetAttribute(fomo::batch_stress_kernel<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s));
+        g_batch_smem[1][M] = s;
+    }
+    return FOMO_OK;
+}
+
+int set_batch_smem(int M, size_t v, size_t s) {
+    switch (M) {
+        case 1: return set_batch_smem_M<1>(v, s);
+        case 2: return set_batch_smem_M<2>(v, s);
+        case 3: return set_batch_smem_M<3>(v, s);
+        case 4: return set_batch_smem_M<4>(v, s);
+        case 5: return set_batch_smem_M<5>(v, s);
+        case 6: return set_batch_smem_M<6>(v, s);
+    }
+    return fail(FOMO_EINVAL, "M=%d not supported", M);
+}
+
+template <int M>
+void launch_batch_M(bool vel, const fomo::BatchArgs& B, int grid, size_t smem, cudaStream_t st) {
+    if (vel) fomo::batch_velocity_kernel<M><<<grid, fomo::kThreads, smem, st>>>(B);
+    else fomo::batch_stress_kernel<M><<<grid, fomo::kThreads, smem, st>>>(B);
+}
+
+void launch_batch(int M, bool vel, const fomo::BatchArgs& B, int grid, size_t smem, cudaStream_t st) {
+    switch (M) {
+        case 1: launch_batch_M<1>(vel, B, grid, smem, st); break;
+        case 2: launch_batch_M<2>(vel, B, grid, smem, st); break;
+        case 3: launch_batch_M<3>(vel, B, grid, smem, st); break;
+        case 4: launch_batch_M<4>(vel, B, grid, smem, st); break;
+        case 5: launch_batch_M<5>(vel, B, grid, smem, st); break;
+        case 6: launch_batch_M<6>(vel, B, grid, smem, st); break;
+    }
+}
+
+// The shots of one FD order in flight: one velocity and one stress launch.
+struct LaunchSet {
+    int M = 0;
+    fomo::BatchArgs args{};
+    int grid_v = 0, grid_s = 0;
+    size_t smem_v = 0, smem_s = 0;
+};
+
+class Server {
+  public:
+    explicit Server(const FomoServerConfig& cfg) : cfg_(cfg) {}
+
+    int start(int device) {
+        device_ = device;
+        CUDA_TRY(cudaSetDevice(device));
+        CUDA_TRY(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking));
+        cudaMemPoolProps props;
+        std::memset(&props, 0, sizeof(props));
+        props.allocType = cudaMemAllocationTypePinned;
+        props.handleTypes = cudaMemHandleTypeNone;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = device;
+        CUDA_TRY(cudaMemPoolCreate(&pool_, &props));
+        uint64_t keep = UINT64_MAX;
+        CUDA_TRY(cudaMemPoolSetAttribute(pool_, cudaMemPoolAttrReleaseThreshold, &keep));
+        CUDA_TRY(cudaMalloc(&d_ctl_, 256));
+        d_step_ = reinterpret_cast<int*>(d_ctl_);
+        d_status_ = reinterpret_cast<int*>(d_ctl_ + 128);
+        const int one = 1;
+        CUDA_TRY(cudaMemcpy(d_step_, &one, sizeof(int), cudaMemcpyHostToDevice));
+        CUDA_TRY(cudaMemset(d_status_, 0, sizeof(int)));
+        if (cfg_.hbm_budget_bytes == 0) {
+            size_t fr = 0, tot = 0;
+            CUDA_TRY(cudaMemGetInfo(&fr, &tot));
+            budget_ = (size_t)(0.9 * (double)fr);
+        } else {
+            budget_ = cfg_.hbm_budget_bytes;
+        }
+        worker_ = std::thread([this] { loop(); });
+        return FOMO_OK;
+    }
+
+    ~Server() { shutdown(); }
+
+    void shutdown() {
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            if (stopped_) return;
+            stopping_ = true;
+            for (auto& r : queue_) finish_locked(*r, kCancelled, FOMO_ECANCELLED, "server destroyed before the shot ran");
+            queue_.clear();
+        }
+        cv_work_.notify_all();
+        if (worker_.joinable()) worker_.join();
+        cudaSetDevice(device_);
+        if (st_) cudaStreamSynchronize(st_);
+        for (auto& g : graphs_) cudaGraphExecDestroy(g.second);
+        graphs_.clear();
+        for (auto& d : deferred_) {
+            if (d.exec) cudaGraphExecDestroy(d.exec);
+            if (d.ev) cudaEventDestroy(d.ev);
+        }
+        deferred_.clear();
+        for (auto e : ev_free_) cudaEventDestroy(e);
+        ev_free_.clear();
+        for (auto e : tev_free_) cudaEventDestroy(e);
+        tev_free_.clear();
+        if (d_tables_ && st_) cudaFreeAsync(d_tables_, st_);
+        d_tables_ = nullptr;
+        if (st_) cudaStreamSynchronize(st_);
+        if (d_ctl_) cudaFree(d_ctl_);
+        d_ctl_ = nullptr;
+        if (pool_) cudaMemPoolDestroy(pool_);
+        pool_ = nullptr;
+        if (st_) cudaStreamDestroy(st_);
+        st_ = nullptr;
+        std::lock_guard<std::mutex> lk(mu_);
+        stopped_ = true;
+        cv_done_.notify_all();
+    }
+
+    int submit(std::shared_ptr<Request> r, uint64_t* ticket) {
+        std::lock_guard<std::mutex> lk(mu_);
+        if (stopping_) return fail(FOMO_EINVAL, "server is shutting down");
+        if (!error_.empty()) return fail(FOMO_ECUDA, "server failed: %s", error_.c_str());
+        if (r->bytes + r->buoy_bytes > budget_)
+            return fail(FOMO_ENOMEM, "shot needs %zu device bytes, more than the server's HBM budget of %zu",
+                        r->bytes + r->buoy_bytes, budget_);
+        r->ticket = next_ticket_++;
+        r->t_submit = Clock::now();
+        reqs_[r->ticket] = r;
+        queue_.push_back(r);
+        stats_.submitted += 1;
+        *ticket = r->ticket;
+        cv_work_.notify_all();
+        return FOMO_OK;
+    }
+
+    int poll(uint64_t ticket, int32_t* done) {
+        std::lock_guard<std::mutex> lk(mu_);
+        auto it = reqs_.find(ticket);
+        if (it == reqs_.end()) return fail(FOMO_EINVAL, "unknown ticket %llu", (unsigned long long)ticket);
+        const Request& r = *it->second;
+        *done = r.state >= kDone ? 1 : 0;
+        if (r.state >= kFailed) return fail(r.rc, "%s", r.err.c_str());
+        return FOMO_OK;
+    }
+
+    int wait(uint64_t ticket, double timeout_s, FomoRequestStats* stats) {
+        std::unique_lock<std::mutex> lk(mu_);
+        auto it = reqs_.find(ticket);
+        if (it == reqs_.end()) return fail(FOMO_EINVAL, "unknown ticket %llu", (unsigned long long)ticket);
+        std::shared_ptr<Request> r = it->second;
+        auto ready = [&] { return r->state >= kDone; };
+        if (timeout_s < 0) {
+            cv_done_.wait(lk, ready);
+        } else if (!cv_done_.wait_for(lk, std::chrono::duration<double>(timeout_s), ready)) {
+            return fail(FOMO_ENOTREADY, "request %llu not finished after %.3f s", (unsigned long long)ticket, timeout_s);
+        }
+        if (stats) {
+            std::memset(stats, 0, sizeof(*stats));
+            const bool admitted = r->t_admit.time_since_epoch().count() != 0;
+            stats->queue_ms = admitted ? ms_between(r->t_submit, r->t_admit) : 0;
+            stats->run_ms = admitted ? ms_between(r->t_admit, r->t_done) : 0;
+            stats->latency_ms = ms_between(r->t_submit, r->t_done);
+            stats->steps = r->state == kDone ? r->nt : 0;
+            stats->batch_peak = r->batch_peak;
+        }
+        reqs_.erase(ticket);
+        if (r->state != kDone) return fail(r->rc, "%s", r->err.c_str());
+        return FOMO_OK;
+    }
+
+    int cancel(uint64_t ticket) {
+        std::lock_guard<std::mutex> lk(mu_);
+        auto it = reqs_.find(ticket);
+        if (it == reqs_.end()) return fail(FOMO_EINVAL, "unknown ticket %llu", (unsigned long long)ticket);
+        Request& r = *it->second;
+        if (r.state != kQueued) return fail(FOMO_EINVAL, "request %llu is not queued", (unsigned long long)ticket);
+        for (auto q = queue_.begin(); q != queue_.end(); ++q)
+            if ((*q)->ticket == ticket) {
+                queue_.erase(q);
+                break;
+            }
+        finish_locked(r, kCancelled, FOMO_ECANCELLED, "request cancelled");
+        return FOMO_OK;
+    }
+
+    void get_stats(FomoServerStats* s) {
+        std::lock_guard<std::mutex> lk(mu_);
+        *s = stats_;
+    }
+
+    cudaStream_t stream() const { return st_; }
+
+  private:
+    struct Deferred {  // released once `ev` has completed
+        cudaEvent_t ev = nullptr;
+        cudaGraphExec_t exec = nullptr;
+        void* pinned = nullptr;
+    };
+    struct Measure {   // a timed chunk of the autotuner
+        TuneKey key;
+        int cand;
+        int steps;
+        cudaEvent_t a, b;
+    };
+
+    FomoServerConfig cfg_;
+    int device_ = 0;
+    size_t budget_ = 0;
+    cudaStream_t st_ = nullptr;
+    cudaMemPool_t pool_ = nullptr;
+    unsigned char* d_ctl_ = nullptr;
+    int* d_step_ = nullptr;
+    int* d_status_ = nullptr;
+    std::thread worker_;
+
+    std::mutex mu_;
+    std::condition_variable cv_work_, cv_done_;
+    std::deque<std::shared_ptr<Request>> queue_;
+    std::unordered_map<uint64_t, std::shared_ptr<Request>> reqs_;
+    uint64_t next_ticket_ = 1;
+    bool stopping_ = false, stopped_ = false;
+    std::string error_;
+    FomoServerStats stats_{};
+
+    // Worker only.
+    std::vector<std::shared_ptr<Request>> active_;
+    std::vector<std::shared_ptr<Request>> retiring_;
+    std::map<std::tuple<Medium*, uint32_t, uint32_t>, std::unique_ptr<Resident>> resident_;
+    size_t used_ = 0;
+    int64_t k_host_ = 0;          // batch steps enqueued
+    bool dirty_ = true;           // membership changed since the tables were built
+    std::vector<LaunchSet> sets_;
+    unsigned char* d_tables_ = nullptr;
+    std::map<int, cudaGraphExec_t> graphs_;  // K -> graph of the current tables
+    std::deque<cudaEvent_t> inflight_;
+    std::vector<Deferred> deferred_;
+    std::vector<Measure> measures_;
+    std::vector<cudaEvent_t> ev_free_, tev_free_;
+    PinnedPool pinned_;
+
+    // ------------------------------------------------------------ helpers
+    cudaEvent_t event(bool timing = false) {
+        auto& fl = timing ? tev_free_ : ev_free_;
+        if (!fl.empty()) {
+            cudaEvent_t e = fl.back();
+            fl.pop_back();
+            return e;
+        }
+        cudaEvent_t e = nullptr;
+        cudaEventCreateWithFlags(&e, timing ? cudaEventDefault : cudaEventDisableTiming);
+        return e;
+    }
+    void release_event(cudaEvent_t e, bool timing = false) { (timing ? tev_free_ : ev_free_).push_back(e); }
+
+    static std::tuple<Medium*, uint32_t, uint32_t> res_key(const Request& r) {
+        uint32_t bx, bz;
+        std::memcpy(&bx, &r.dtx, 4);
+        std::memcpy(&bz, &r.dtz, 4);
+        return std::make_tuple(r.med, bx, bz);
+    }
+
+    void finish_locked(Request& r, int state, int rc, const std::string& msg) {
+        r.state = state;
+        r.rc = rc;
+        r.err = msg;
+        r.t_done = Clock::now();
+        if (state == kDone) stats_.completed += 1;
+        else if (state == kFailed) stats_.failed += 1;
+        else if (state == kCancelled) stats_.cancelled += 1;
+        if (r.med) {
+            r.med->users.fetch_sub(1);
+            r.med = nullptr;
+        }
+        cv_done_.notify_all();
+    }
+
+    // A CUDA failure in the worker fails every request it holds and stops
+    // admission; the server must then be destroyed.
+    void fatal(const std::string& msg) {
+        cudaStreamSynchronize(st_);
+        std::lock_guard<std::mutex> lk(mu_);
+        if (error_.empty()) error_ = msg.empty() ? std::string("batch loop failed") : msg;
+        for (auto& r : active_) finish_locked(*r, kFailed, FOMO_ECUDA, error_);
+        for (auto& r : retiring_) finish_locked(*r, kFailed, FOMO_ECUDA, error_);
+        for (auto& r : queue_) finish_locked(*r, kFailed, FOMO_ECUDA, error_);
+        active_.clear();
+        retiring_.clear();
+        queue_.clear();
+    }
+
+    void count_launches(int64_t n) {
+        std::lock_guard<std::mutex> lk(mu_);
+        stats_.kernel_launches += n;
+    }
+
+    // ------------------------------------------------------------ admission
+    Resident* resident_for(Request& r, int* rc) {
+        *rc = FOMO_OK;
+        auto key = res_key(r);
+        auto it = resident_.find(key);
+        if (it != resident_.end()) return it->second.get();
+        auto R = std::make_unique<Resident>();
+        Medium& m = *r.med;
+        R->med = r.med;
+        R->dtx = r.dtx;
+        R->dtz = r.dtz;
+        R->iso = r.dtx == r.dtz ? 1 : 0;
+        const size_t plane = (size_t)m.pitch * m.nz;
+        R->bytes = (R->iso ? 2 : 4) * plane * sizeof(float);
+        if (cudaMallocFromPoolAsync(reinterpret_cast<void**>(&R->buoy), R->bytes, pool_, st_) != cudaSuccess) {
+            *rc = fail(FOMO_ENOMEM, "buoyancy allocation of %zu bytes failed", R->bytes);
+            return nullptr;
+        }
+        float* b0 = R->buoy;
+        float* b2 = R->buoy + plane;
+        float* b1 = R->iso ? b0 : R->buoy + 2 * plane;
+        float* b3 = R->iso ? b2 : R->buoy + 3 * plane;
+        fomo::buoyancy_kernel<<<4 * 148, 256, 0, st_>>>(m.arr(0), m.arr(1), r.dtx, r.dtz, plane, b0, b1, b2, b3);
+        if (cudaGetLastError() != cudaSuccess) {
+            *rc = fail(FOMO_ECUDA, "buoyancy kernel launch failed");
+            return nullptr;
+        }
+        count_launches(1);
+        R->b[0] = b0;
+        R->b[1] = b1;
+        R->b[2] = b2;
+        R->b[3] = b3;
+        for (int q = 0; q < 4; ++q)
+            if ((*rc = encode_map(&R->bmap[q], R->b[q], m.nx, m.nz, m.pitch, fomo::kTX, fomo::kTZ))) return nullptr;
+        for (int q = 0; q < 3; ++q)
+            if ((*rc = encode_map(&R->mod[q], m.arr(2 + q), m.nx, m.nz, m.pitch, fomo::kTX, fomo::kTZ))) return nullptr;
+        used_ += R->bytes;
+        Resident* p = R.get();
+        resident_.emplace(key, std::move(R));
+        return p;
+    }
+
+    template <int M>
+    int build_maps(Request& r, float* const (&field)[2][5]) {
+        using G = fomo::Geo<M>;
+        const Medium& m = *r.med;
+        CUtensorMap halo[2][5], tile[2][5];
+        for (int c = 0; c < 2; ++c)
+            for (int q = 0; q < 5; ++q) {
+                if (int rc = encode_map(&halo[c][q], field[c][q], m.nx, m.nz, m.pitch, G::BOXW, G::BOXH)) return rc;
+                if (int rc = encode_map(&tile[c][q], field[c][q], m.nx, m.nz, m.pitch, fomo::kTX, fomo::kTZ)) return rc;
+            }
+        const Resident& R = *r.res;
+        for (int a = 0; a < 2; ++a) {
+            const int b = 1 - a;
+            fomo::VelMaps& vm = r.dev.vmap[a];
+            vm.xx = halo[a][fomo::TXX];
+            vm.zz = halo[a][fomo::TZZ];
+            vm.xz = halo[a][fomo::TXZ];
+            vm.vx = tile[a][fomo::VX];
+            vm.vz = tile[a][fomo::VZ];
+            vm.b0 = R.bmap[0];
+            vm.b1 = R.bmap[1];
+            vm.b2 = R.bmap[2];
+            vm.b3 = R.bmap[3];
+            fomo::StrMaps& sm = r.dev.smap[a];
+            sm.vx = halo[b][fomo::VX];
+            sm.vz = halo[b][fomo::VZ];
+            sm.txx = tile[a][fomo::TXX];
+            sm.tzz = tile[a][fomo::TZZ];
+            sm.txz = tile[a][fomo::TXZ];
+            sm.lam = R.mod[0];
+            sm.mu = R.mod[1];
+            sm.mxz = R.mod[2];
+        }
+        return FOMO_OK;
+    }
+
+    int build_maps_any(Request& r, float* const (&field)[2][5]) {
+        switch (r.M) {
+            case 1: return build_maps<1>(r, field);
+            case 2: return build_maps<2>(r, field);
+            case 3: return build_maps<3>(r, field);
+            case 4: return build_maps<4>(r, field);
+            case 5: return build_maps<5>(r, field);
+            case 6: return build_maps<6>(r, field);
+        }
+        return fail(FOMO_EINVAL, "M=%d not supported", r.M);
+    }
+
+    static Launch shape_of(const Request& r) {
+        const Medium& m = *r.med;
+        Launch L;
+        L.tiles_x = (m.nx + fomo::kTX - 1) / fomo::kTX;
+        L.tiles_z = (m.nz + fomo::kTZ - 1) / fomo::kTZ;
+        L.x_last = std::max(0, (m.nx + 3) / 4 * 4 - fomo::kTX);
+        L.n_tile = L.tiles_x * L.tiles_z;
+        L.n_band = fomo::band_block_count(m.nx);
+        const bool iso = r.dtx == r.dtz;
+        L.smem_v = batch_smem_any(r.M, true, r.nbc, iso);
+        L.smem_s = batch_smem_any(r.M, false, r.nbc, iso);
+        return L;
+    }
+
+    // Bytes of the pinned upload area of a shot.
+    static size_t stage_bytes(const Request& r) {
+        return align_up(r.tabs.size() * 4, 256) + align_up(r.cells.size() * 4, 256) +
+               align_up(std::max<size_t>(r.wavelet.size(), 1) * 4, 256);
+    }
+
+    // Allocates and uploads an admitted shot; `stage` is pinned memory for the
+    // uploads (released with the chunk that follows).
+    int admit(Request& r, unsigned char* stage) {
+        int rc = FOMO_OK;
+        r.res = resident_for(r, &rc);
+        if (!r.res) return rc;
+        r.res->refs += 1;
+        const Medium& m = *r.med;
+        const size_t plane = (size_t)m.pitch * m.nz * sizeof(float);
+        r.tabs_off = 10 * plane;
+        r.cells_off = r.tabs_off + align_up(r.tabs.size() * 4, 256);
+        r.wav_off = r.cells_off + align_up(r.cells.size() * 4, 256);
+        r.gather_off = r.wav_off + align_up(std::max<size_t>(r.wavelet.size(), 1) * 4, 256);
+        const size_t total = r.gather_off + align_up((size_t)r.nt * r.n_rec * 4, 256);
+        if (cudaMallocFromPoolAsync(reinterpret_cast<void**>(&r.d_block), total, pool_, st_) != cudaSuccess)
+            return fail(FOMO_ENOMEM, "shot allocation of %zu bytes failed", total);
+        r.bytes = total;
+        used_ += total;
+        unsigned char* base = r.d_block;
+        CUDA_TRY(cudaMemsetAsync(base, 0, 10 * plane, st_));
+        std::memcpy(stage, r.tabs.data(), r.tabs.size() * 4);
+        std::memcpy(stage + (r.cells_off - r.tabs_off), r.cells.data(), r.cells.size() * 4);
+        std::memcpy(stage + (r.wav_off - r.tabs_off), r.wavelet.data(), r.wavelet.size() * 4);
+        CUDA_TRY(cudaMemcpyAsync(base + r.tabs_off, stage, r.gather_off - r.tabs_off, cudaMemcpyHostToDevice, st_));
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            stats_.h2d_bytes += (int64_t)(r.gather_off - r.tabs_off);
+        }
+        r.d_gather = reinterpret_cast<float*>(base + r.gather_off);
+        float* field[2][5];
+        for (int c = 0; c < 2; ++c)
+            for (int q = 0; q < 5; ++q) field[c][q] = reinterpret_cast<float*>(base + (size_t)(c * 5 + q) * plane);
+        if (int e = build_maps_any(r, field)) return e;
+
+        fomo::StepParams& P = r.dev.P;
+        std::memset(&P, 0, sizeof(P));
+        P.nx = m.nx;
+        P.nz = m.nz;
+        P.pitch = m.pitch;
+        P.M = m.M;
+        P.pad = m.pad;
+        P.nbc = r.nbc;
+        P.fs = m.fs;
+        P.dtx = r.dtx;
+        P.dtz = r.dtz;
+        for (int l = 0; l < fomo::kMaxM; ++l) P.a[l] = r.a[l];
+        P.qx = r.q[0];
+        P.qz = r.q[1];
+        P.qt_x = r.q[2];
+        P.qt_z = r.q[3];
+        P.qxt = r.q[4];
+        const float* tabs = reinterpret_cast<const float*>(base + r.tabs_off);
+        for (int t = 0; t < 3; ++t) P.w_tab[t] = tabs + (size_t)t * (r.nbc + 2);
+        P.rho_vx = m.arr(0);
+        P.rho_vz = m.arr(1);
+        P.lam = m.arr(2);
+        P.mu_txx = m.arr(3);
+        P.mu_txz = m.arr(4);
+        P.src_i = r.src_i;
+        P.src_j = r.src_j;
+        P.nt = r.nt;
+        P.n_rec = r.n_rec;
+        P.rec_kind = r.rec_kind;
+        P.rec_cell = reinterpret_cast<const int*>(base + r.cells_off);
+        P.gather = r.d_gather;
+        const Launch L = shape_of(r);
+        fomo::TiledArgs& T = r.dev.T;
+        std::memset(&T, 0, sizeof(T));
+        for (int q = 0; q < 4; ++q) T.b[q] = r.res->b[q];
+        T.iso = r.res->iso;
+        T.status = d_status_;
+        T.n_band_blocks = L.n_band;
+        T.n_tile_blocks = L.n_tile;
+        T.tiles_x = L.tiles_x;
+        T.x_last = L.x_last;
+        for (int c = 0; c < 2; ++c)
+            for (int q = 0; q < 5; ++q) r.dev.field[c][q] = field[c][q];
+        r.dev.wavelet = reinterpret_cast<const float*>(base + r.wav_off);
+        r.dev.n_wavelet = (int)r.wavelet.size();
+        r.start = (int)(k_host_ + 1);
+        r.dev.start = r.start;
+        r.dev.nt = r.nt;
+        return FOMO_OK;
+    }
+
+    // ------------------------------------------------------------ tables
+    int build_tables() {
+        // Order: by M, then by medium (groups), then admission.
+        std::vector<Request*> order;
+        for (auto& r : active_) order.push_back(r.get());
+        std::stable_sort(order.begin(), order.end(), [](const Request* x, const Request* y) {
+            if (x->M != y->M) return x->M < y->M;
+            return x->med < y->med;
+        });
+        sets_.clear();
+        struct Part {
+            size_t shots_off = 0, groups_off = 0, rec_off = 0;
+            std::vector<fomo::GroupDev> groups;
+            std::vector<int> rec;
+            size_t n0 = 0, n = 0;
+        };
+        std::vector<Part> parts;
+        size_t bytes = 0;
+        for (size_t i = 0; i < order.size();) {
+            size_t j = i;
+            while (j < order.size() && order[j]->M == order[i]->M) ++j;
+            Part p;
+            p.n0 = i;
+            p.n = j - i;
+            LaunchSet S;
+            S.M = order[i]->M;
+            int band = 0, tile = 0;
+            for (size_t g = i; g < j;) {
+                size_t h = g;
+                while (h < j && order[h]->med == order[g]->med) ++h;
+                const Launch L = shape_of(*order[g]);
+                fomo::GroupDev G;
+                G.first = (int)(g - i);
+                G.n = (int)(h - g);
+                G.n_band = L.n_band;
+                G.n_tile = L.n_tile;
+                G.band_off = band;
+                G.tile_off = tile;
+                band += G.n * G.n_band;
+                tile += G.n * G.n_tile;
+                p.groups.push_back(G);
+                g = h;
+            }
+            int rec = 0;
+            p.rec.push_back(0);
+            for (size_t k = i; k < j; ++k) {
+                const Request& r = *order[k];
+                rec += (r.n_rec + fomo::kThreads - 1) / fomo::kThreads;
+                p.rec.push_back(rec);
+                const Launch L = shape_of(r);
+                S.smem_v = std::max(S.smem_v, L.smem_v);
+                S.smem_s = std::max(S.smem_s, L.smem_s);
+            }
+            S.args.n_shots = (int)p.n;
+            S.args.n_groups = (int)p.groups.size();
+            S.args.total_band = band;
+            S.args.total_tile = tile;
+            S.grid_v = band + tile + rec;
+            S.grid_s = band + tile;
+            p.shots_off = bytes;
+            bytes += align_up(p.n * sizeof(fomo::ShotDev), 256);
+            p.groups_off = bytes;
+            bytes += align_up(p.groups.size() * sizeof(fomo::GroupDev), 256);
+            p.rec_off = bytes;
+            bytes += align_up(p.rec.size() * sizeof(int), 256);
+            parts.push_back(std::move(p));
+            sets_.push_back(S);
+            i = j;
+        }
+        // Replace the device tables (stream ordered: launches already queued
+        // keep reading the old ones until they are done).
+        if (d_tables_) CUDA_TRY(cudaFreeAsync(d_tables_, st_));
+        d_tables_ = nullptr;
+        retire_graphs();
+        if (sets_.empty()) return FOMO_OK;
+        if (cudaMallocFromPoolAsync(reinterpret_cast<void**>(&d_tables_), bytes, pool_, st_) != cudaSuccess)
+            return fail(FOMO_ENOMEM, "batch table allocation of %zu bytes failed", bytes);
+        unsigned char* h = static_cast<unsigned char*>(pinned_.take(bytes));
+        if (!h) return fail(FOMO_ENOMEM, "pinned staging of %zu bytes failed", bytes);
+        for (size_t s = 0; s < parts.size(); ++s) {
+            const Part& p = parts[s];
+            fomo::ShotDev* sd = reinterpret_cast<fomo::ShotDev*>(h + p.shots_off);
+            for (size_t k = 0; k < p.n; ++k)
+                std::memcpy((void*)&sd[k], (const void*)&order[p.n0 + k]->dev, sizeof(fomo::ShotDev));
+            std::memcpy(h + p.groups_off, p.groups.data(), p.groups.size() * sizeof(fomo::GroupDev));
+            std::memcpy(h + p.rec_off, p.rec.data(), p.rec.size() * sizeof(int));
+            LaunchSet& S = sets_[s];
+            S.args.shots = reinterpret_cast<const fomo::ShotDev*>(d_tables_ + p.shots_off);
+            S.args.groups = reinterpret_cast<const fomo::GroupDev*>(d_tables_ + p.groups_off);
+            S.args.rec_off = reinterpret_cast<const int*>(d_tables_ + p.rec_off);
+            S.args.step = d_step_;
+            if (int rc = set_batch_smem(S.M, S.smem_v, S.smem_s)) return rc;
+        }
+        CUDA_TRY(cudaMemcpyAsync(d_tables_, h, bytes, cudaMemcpyHostToDevice, st_));
+        Deferred d;
+        d.ev = event();
+        d.pinned = h;
+        CUDA_TRY(cudaEventRecord(d.ev, st_));
+        deferred_.push_back(d);
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            stats_.h2d_bytes += (int64_t)bytes;
+        }
+        dirty_ = false;
+        return FOMO_OK;
+    }
+
+    // Graphs of the old tables are destroyed once the launches queued so far
+    // are done.
+    void retire_graphs() {
+        for (auto& g : graphs_) {
+            Deferred d;
+            d.ev = event();
+            d.exec = g.second;
+            cudaEventRecord(d.ev, st_);
+            deferred_.push_back(d);
+        }
+        graphs_.clear();
+    }
+
+    // ------------------------------------------------------------ stepping
+    int launches_per_step() const { return 2 * (int)sets_.size() + 1; }
+
+    void enqueue_step() {
+        for (const LaunchSet& S : sets_) launch_batch(S.M, true, S.args, S.grid_v, S.smem_v, st_);
+        for (const LaunchSet& S : sets_) launch_batch(S.M, false, S.args, S.grid_s, S.smem_s, st_);
+        fomo::batch_advance_kernel<<<1, 1, 0, st_>>>(d_step_);
+    }
+
+    int graph_for(int K, cudaGraphExec_t* out) {
+        auto it = graphs_.find(K);
+        if (it != graphs_.end()) {
+            *out = it->second;
+            return FOMO_OK;
+        }
+        cudaGraph_t g = nullptr;
+        CUDA_TRY(cudaStreamBeginCapture(st_, cudaStreamCaptureModeThreadLocal));
+        for (int k = 0; k < K; ++k) enqueue_step();
+        cudaError_t e = cudaStreamEndCapture(st_, &g);
+        if (e != cudaSuccess) return fail(FOMO_ECUDA, "graph capture failed: %s", cudaGetErrorString(e));
+        cudaGraphExec_t x = nullptr;
+        e = cudaGraphInstantiate(&x, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) return fail(FOMO_ECUDA, "graph instantiation failed: %s", cudaGetErrorString(e));
+        graphs_[K] = x;
+        *out = x;
+        return FOMO_OK;
+    }
+
+    TuneKey tune_key() const {
+        // The largest medium in flight names the batch.
+        const Request* big = active_.front().get();
+        for (auto& r : active_)
+            if ((double)r->med->nx * r->med->nz > (double)big->med->nx * big->med->nz) big = r.get();
+        int n = (int)active_.size(), lg = 0;
+        while ((1 << (lg + 1)) <= n) ++lg;
+        return TuneKey{big->med->nx, big->med->nz, big->M, lg};
+    }
+
+    // Candidate index of the next chunk: the cached choice, else the first
+    // candidate neither measured nor being measured for this key.
+    int choose(const TuneKey& key, bool* measure) {
+        *measure = false;
+        if (cfg_.steps_per_launch > 0) {
+            for (int c = 0; c < 3; ++c)
+                if (kTuneK[c] == cfg_.steps_per_launch) return c;
+            return -2;  // a K outside the candidates: graphs of exactly that K
+        }
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        TuneEntry& e = g_tune[key];
+        if (e.chosen >= 0) return e.chosen;
+        for (int c = 0; c < 3; ++c)
+            if (e.ms_per_step[c] < 0) {
+                bool pending = false;
+                for (auto& m : measures_)
+                    if (!(m.key < key) && !(key < m.key) && m.cand == c) pending = true;
+                if (!pending) {
+                    *measure = true;
+                    return c;
+                }
+            }
+        return 1;  // all measured or pending: K = 8 meanwhile
+    }
+
+    void resolve_measures(bool block) {
+        for (size_t i = 0; i < measures_.size();) {
+            Measure& m = measures_[i];
+            if (block) cudaEventSynchronize(m.b);
+            if (cudaEventQuery(m.b) != cudaSuccess) {
+                ++i;
+                continue;
+            }
+            float ms = 0;
+            cudaEventElapsedTime(&ms, m.a, m.b);
+            {
+                std::lock_guard<std::mutex> lk(g_tune_mu);
+                TuneEntry& e = g_tune[m.key];
+                e.ms_per_step[m.cand] = ms / m.steps;
+                bool all = true;
+                int best = 0;
+                for (int c = 0; c < 3; ++c) {
+                    if (e.ms_per_step[c] < 0) all = false;
+                    else if (e.ms_per_step[best] < 0 || e.ms_per_step[c] < e.ms_per_step[best]) best = c;
+                }
+                if (all && e.chosen < 0) e.chosen = best;
+            }
+            release_event(m.a, true);
+            release_event(m.b, true);
+            measures_.erase(measures_.begin() + i);
+        }
+    }
+
+    int run_chunk() {
+        int64_t rem = INT64_MAX;
+        for (auto& r : active_) rem = std::min<int64_t>(rem, (int64_t)r->start + r->nt - 1 - k_host_);
+        const TuneKey key = tune_key();
+        bool measure = false;
+        const int cand = choose(key, &measure);
+        const int K = cand >= 0 ? kTuneK[cand] : cfg_.steps_per_launch;
+        const int chunk = K == 1 ? kPlainChunk : K;
+        const int n = (int)std::min<int64_t>(chunk, rem);
+        const bool graph = K > 1 && n == K;
+        if (n != chunk) measure = false;
+        cudaGraphExec_t x = nullptr;
+        if (graph)
+            if (int rc = graph_for(K, &x)) return rc;
+        Measure ms{};
+        if (measure) {
+            ms.key = key;
+            ms.cand = cand;
+            ms.steps = n;
+            ms.a = event(true);
+            ms.b = event(true);
+            CUDA_TRY(cudaEventRecord(ms.a, st_));
+        }
+        if (graph) {
+            CUDA_TRY(cudaGraphLaunch(x, st_));
+        } else {
+            for (int k = 0; k < n; ++k) enqueue_step();
+            CUDA_TRY(cudaGetLastError());
+        }
+        if (measure) {
+            CUDA_TRY(cudaEventRecord(ms.b, st_));
+            measures_.push_back(ms);
+        }
+        k_host_ += n;
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            stats_.batch_steps += n;
+            stats_.kernel_launches += (int64_t)n * launches_per_step();
+            if (graph) stats_.graph_replays += 1;
+            stats_.steps_per_launch = graph ? K : 1;
+            const int na = (int)active_.size();
+            for (auto& r : active_) r->batch_peak = std::max(r->batch_peak, na);
+        }
+        cudaEvent_t e = event();
+        CUDA_TRY(cudaEventRecord(e, st_));
+        inflight_.push_back(e);
+        return FOMO_OK;
+    }
+
+    // ------------------------------------------------------------ retirement
+    int retire_done() {
+        bool any = false;
+        for (size_t i = 0; i < active_.size();) {
+            Request& r = *active_[i];
+            if ((int64_t)r.start + r.nt - 1 > k_host_) {
+                ++i;
+                continue;
+            }
+            if (int rc = retire(r)) return rc;
+            retiring_.push_back(active_[i]);
+            active_.erase(active_.begin() + i);
+            any = true;
+        }
+        if (any) dirty_ = true;
+        return FOMO_OK;
+    }
+
+    int retire(Request& r) {
+        const size_t gbytes = (size_t)r.nt * r.n_rec * sizeof(float);
+        if (r.n_rec > 0 && r.nt > 0) {  // receivers of the last step
+            fomo::StepParams P = r.dev.P;
+            const int c = r.nt & 1;  // copy written by step nt
+            for (int q = 0; q < 5; ++q) P.in[q] = r.dev.field[c][q];
+            P.rec_k = r.nt;
+            fomo::record_kernel<<<(r.n_rec + fomo::kThreads - 1) / fomo::kThreads, fomo::kThreads, 0, st_>>>(P);
+            CUDA_TRY(cudaGetLastError());
+            count_launches(1);
+        }
+        r.staging = pinned_.take(gbytes + 16);
+        if (!r.staging) return fail(FOMO_ENOMEM, "pinned staging of %zu bytes failed", gbytes + 16);
+        if (gbytes) CUDA_TRY(cudaMemcpyAsync(r.staging, r.d_gather, gbytes, cudaMemcpyDeviceToHost, st_));
+        CUDA_TRY(cudaMemcpyAsync(static_cast<unsigned char*>(r.staging) + align_up(gbytes, 16), d_status_, sizeof(int),
+                                 cudaMemcpyDeviceToHost, st_));
+        CUDA_TRY(cudaFreeAsync(r.d_block, st_));
+        r.d_block = nullptr;
+        r.done_ev = event();
+        CUDA_TRY(cudaEventRecord(r.done_ev, st_));
+        used_ -= r.bytes;
+        Resident* R = r.res;
+        r.res = nullptr;
+        if (R && --R->refs == 0) {
+            CUDA_TRY(cudaFreeAsync(R->buoy, st_));
+            used_ -= R->bytes;
+            for (auto it = resident_.begin(); it != resident_.end(); ++it)
+                if (it->second.get() == R) {
+                    resident_.erase(it);
+                    break;
+                }
+        }
+        std::lock_guard<std::mutex> lk(mu_);
+        stats_.d2h_bytes += (int64_t)gbytes;
+        return FOMO_OK;
+    }
+
+    // Hands over the gathers whose copies have landed.
+    void complete_retired(bool block) {
+        for (size_t i = 0; i < retiring_.size();) {
+            Request& r = *retiring_[i];
+            if (block) cudaEventSynchronize(r.done_ev);
+            if (cudaEventQuery(r.done_ev) != cudaSuccess) {
+                ++i;
+                continue;
+            }
+            const size_t gbytes = (size_t)r.nt * r.n_rec * sizeof(float);
+            int status = 0;
+            std::memcpy(&status, static_cast<unsigned char*>(r.staging) + align_up(gbytes, 16), sizeof(int));
+            if (!status && gbytes) std::memcpy(r.gather_out, r.staging, gbytes);
+            pinned_.give(r.staging);
+            r.staging = nullptr;
+            release_event(r.done_ev);
+            r.done_ev = nullptr;
+            {
+                std::lock_guard<std::mutex> lk(mu_);
+                if (status == fomo::kErrTmaTimeout)
+                    finish_locked(r, kFailed, FOMO_ETIMEOUT, "a TMA load of a batch time-step kernel did not complete");
+                else if (status)
+                    finish_locked(r, kFailed, FOMO_ECUDA, "batch time-step kernel reported error " + std::to_string(status));
+                else
+                    finish_locked(r, kDone, FOMO_OK, "");
+            }
+            retiring_.erase(retiring_.begin() + i);
+        }
+    }
+
+    void release_deferred(bool block) {
+        for (size_t i = 0; i < deferred_.size();) {
+            Deferred& d = deferred_[i];
+            if (block) cudaEventSynchronize(d.ev);
+            if (cudaEventQuery(d.ev) != cudaSuccess) {
+                ++i;
+                continue;
+            }
+            if (d.exec) cudaGraphExecDestroy(d.exec);
+            if (d.pinned) pinned_.give(d.pinned);
+            release_event(d.ev);
+            deferred_.erase(deferred_.begin() + i);
+        }
+    }
+
+    // ------------------------------------------------------------ the loop
+    void loop() {
+        cudaSetDevice(device_);
+        while (true) {
+            complete_retired(false);
+            release_deferred(false);
+            resolve_measures(false);
+            std::vector<std::shared_ptr<Request>> admitted;
+            {
+                std::unique_lock<std::mutex> lk(mu_);
+                if (active_.empty() && queue_.empty()) {
+                    if (stopping_ && retiring_.empty()) break;
+                    if (retiring_.empty() && deferred_.empty()) {
+                        cv_work_.wait(lk, [&] { return stopping_ || !queue_.empty(); });
+                        continue;
+                    }
+                }
+                size_t planned = used_;
+                std::vector<std::tuple<Medium*, uint32_t, uint32_t>> new_res;
+                while (!queue_.empty()) {
+                    Request& r = *queue_.front();
+                    if (cfg_.max_shots > 0 && (int)(active_.size() + admitted.size()) >= cfg_.max_shots) break;
+                    auto key = res_key(r);
+                    const bool have = resident_.count(key) != 0 ||
+                                      std::find(new_res.begin(), new_res.end(), key) != new_res.end();
+                    const size_t need = r.bytes + (have ? 0 : r.buoy_bytes);
+                    if (planned + need > budget_) break;
+                    planned += need;
+                    if (!have) new_res.push_back(key);
+                    r.state = kRunning;
+                    r.t_admit = Clock::now();
+                    admitted.push_back(queue_.front());
+                    queue_.pop_front();
+                }
+            }
+            if (!admitted.empty()) {
+                size_t sb = 0;
+                for (auto& r : admitted) sb += stage_bytes(*r);
+                unsigned char* stage = static_cast<unsigned char*>(pinned_.take(sb));
+                if (!stage) {
+                    for (auto& r : admitted) active_.push_back(r);
+                    fatal("pinned staging allocation failed");
+                    continue;
+                }
+                size_t off = 0;
+                int rc = FOMO_OK;
+                size_t k = 0;
+                for (; k < admitted.size(); ++k) {
+                    auto& r = admitted[k];
+                    if (r->nt == 0) {  // nothing to run: done at once
+                        std::lock_guard<std::mutex> lk(mu_);
+                        finish_locked(*r, kDone, FOMO_OK, "");
+                        continue;
+                    }
+                    active_.push_back(r);
+                    if ((rc = admit(*r, stage + off))) break;
+                    off += stage_bytes(*r);
+                    dirty_ = true;
+                }
+                Deferred d;
+                d.ev = event();
+                d.pinned = stage;
+                cudaEventRecord(d.ev, st_);
+                deferred_.push_back(d);
+                if (rc) {
+                    for (++k; k < admitted.size(); ++k) active_.push_back(admitted[k]);
+                    fatal(g_err);
+                    continue;
+                }
+                std::lock_guard<std::mutex> lk(mu_);
+                stats_.peak_shots = std::max<int32_t>(stats_.peak_shots, (int32_t)active_.size());
+                stats_.peak_bytes = std::max<uint64_t>(stats_.peak_bytes, used_);
+            }
+            if (active_.empty()) {
+                // Nothing to run: wait for copies in flight, then look again.
+                if (!retiring_.empty()) complete_retired(true);
+                else if (!deferred_.empty()) release_deferred(true);
+                continue;
+            }
+            if (dirty_ && build_tables()) {
+                fatal(g_err);
+                continue;
+            }
+            if (run_chunk() || retire_done()) {
+                fatal(g_err);
+                continue;
+            }
+            while (inflight_.size() > 2) {
+                cudaEventSynchronize(inflight_.front());
+                release_event(inflight_.front());
+                inflight_.pop_front();
+            }
+            cudaError_t e = cudaGetLastError();
+            if (e != cudaSuccess) fatal(std::string("CUDA error in the batch loop: ") + cudaGetErrorString(e));
+        }
+        for (auto e : inflight_) {
+            cudaEventSynchronize(e);
+            release_event(e);
+        }
+        inflight_.clear();
+        resolve_measures(true);
+        release_deferred(true);
+    }
+};
+
+struct ServerTable {
+    std::mutex mu;
+    std::unordered_map<uint64_t, std::shared_ptr<Server>> servers;
+    uint64_t next = 1;
+};
+
+ServerTable& servers() {
+    static ServerTable t;
+    return t;
+}
+
+void shutdown_servers() {
+    std::vector<std::shared_ptr<Server>> all;
+    {
+        auto& T = servers();
+        std::lock_guard<std::mutex> lk(T.mu);
+        for (auto& kv : T.servers) all.push_back(kv.second);
+        T.servers.clear();
+    }
+    for (auto& s : all) s->shutdown();
+}
+
+std::shared_ptr<Server> find_server(uint64_t h) {
+    auto& T = servers();
+    std::lock_guard<std::mutex> lk(T.mu);
+    auto it = T.servers.find(h);
+    return it == T.servers.end() ? nullptr : it->second;
+}
+
+// Validates a shot against its medium (the checks of fomo_b200_shot_begin)
+// and copies it into a request.
+int make_request(Medium* m, const FomoHabc* habc, const FomoShot* shot, float* gather_out,
+                 std::shared_ptr<Request>* out) {
+    if (!habc || !shot) return fail(FOMO_EINVAL, "NULL argument");
+    if (shot->M != m->M) return fail(FOMO_EINVAL, "shot M=%d differs from medium M=%d", shot->M, m->M);
+    if (!shot->a) return fail(FOMO_EINVAL, "FD coefficients are NULL");
+    if (shot->nt < 0) return fail(FOMO_EINVAL, "nt=%d < 0", shot->nt);
+    const int nbc = habc->nbc;
+    if (nbc < 1 || 2 * nbc + 3 > m->nx || 2 * nbc + 2 > m->nz)
+        return fail(FOMO_EINVAL, "nbc=%d does not fit the %dx%d grid", nbc, m->nx, m->nz);
+    if (!habc->w_vx || !habc->w_vz || !habc->w_tau) return fail(FOMO_EINVAL, "HABC weight tables are NULL");
+    if (shot->src_i < 1 || shot->src_i > m->nx || shot->src_j < 1 || shot->src_j > m->nz)
+        return fail(FOMO_EINVAL, "source (%d, %d) outside the %dx%d grid", shot->src_i, shot->src_j, m->nx, m->nz);
+    if (shot->n_wavelet < 0 || (shot->n_wavelet > 0 && !shot->wavelet)) return fail(FOMO_EINVAL, "bad wavelet");
+    if (shot->n_rec < 0 || (shot->n_rec > 0 && (!shot->rec_i || !shot->rec_j)))
+        return fail(FOMO_EINVAL, "bad receiver arrays");
+    if (shot->rec_kind < 0 || shot->rec_kind > 2) return fail(FOMO_EINVAL, "bad receiver kind %d", shot->rec_kind);
+    if (shot->n_rec > 0 && shot->nt > 0 && !gather_out) return fail(FOMO_EINVAL, "gather_out is NULL");
+    const bool iso = shot->dtx == shot->dtz;
+    const size_t smem = std::max(batch_smem_any(m->M, true, nbc, iso), batch_smem_any(m->M, false, nbc, iso));
+    if (smem + fomo::kBatchStaticSmem > 227 * 1024)
+        return fail(FOMO_EINVAL, "nbc=%d needs %zu bytes of shared memory per block, more than 227 KB", nbc, smem);
+    auto r = std::make_shared<Request>();
+    r->med = m;
+    r->M = shot->M;
+    r->nbc = nbc;
+    r->nt = shot->nt;
+    r->src_i = shot->src_i - 1;
+    r->src_j = shot->src_j - 1;
+    r->n_rec = shot->n_rec;
+    r->rec_kind = shot->rec_kind;
+    r->q[0] = habc->qx;
+    r->q[1] = habc->qz;
+    r->q[2] = habc->qt_x;
+    r->q[3] = habc->qt_z;
+    r->q[4] = habc->qxt;
+    for (int l = 0; l < shot->M; ++l) r->a[l] = shot->a[l];
+    r->dtx = shot->dtx;
+    r->dtz = shot->dtz;
+    const size_t tab_n = (size_t)nbc + 2;
+    r->tabs.resize(3 * tab_n);
+    std::memcpy(r->tabs.data(), habc->w_vx, tab_n * 4);
+    std::memcpy(r->tabs.data() + tab_n, habc->w_vz, tab_n * 4);
+    std::memcpy(r->tabs.data() + 2 * tab_n, habc->w_tau, tab_n * 4);
+    r->wavelet.assign(shot->wavelet, shot->wavelet + shot->n_wavelet);
+    r->cells.resize(shot->n_rec);
+    for (int k = 0; k < shot->n_rec; ++k) {
+        const int i = shot->rec_i[k], j = shot->rec_j[k];
+        if (i < 1 || i > m->nx || j < 1 || j > m->nz)
+            return fail(FOMO_EINVAL, "receiver %d at (%d, %d) outside the %dx%d grid", k + 1, i, j, m->nx, m->nz);
+        r->cells[k] = (i - 1) + (j - 1) * m->pitch;
+    }
+    r->gather_out = gather_out;
+    const size_t plane = (size_t)m->pitch * m->nz * sizeof(float);
+    r->bytes = 10 * plane + align_up(r->tabs.size() * 4, 256) + align_up(r->cells.size() * 4, 256) +
+               align_up(std::max<size_t>(r->wavelet.size(), 1) * 4, 256) +
+               align_up((size_t)r->nt * r->n_rec * 4, 256);
+    r->buoy_bytes = (iso ? 2 : 4) * plane;
+    *out = std::move(r);
+    return FOMO_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int fomo_b200_server_create(const FomoServerConfig* config, uint64_t* server) {
+    int device = 0;
+    {
+        std::lock_guard<std::mutex> lk(ctx().mu);
+        if (int rc = ensure_init()) return rc;
+        device = ctx().device;
+    }
+    if (!server) return fail(FOMO_EINVAL, "server is NULL");
+    FomoServerConfig cfg{};
+    if (config) cfg = *config;
+    if (cfg.max_shots < 0 || cfg.steps_per_launch < 0 || cfg.steps_per_launch > 1024)
+        return fail(FOMO_EINVAL, "bad server configuration");
+    auto s = std::make_shared<Server>(cfg);
+    if (int rc = s->start(device)) return rc;
+    auto& T = servers();
+    std::lock_guard<std::mutex> lk(T.mu);
+    const uint64_t h = T.next++;
+    T.servers[h] = s;
+    *server = h;
+    return FOMO_OK;
+}
+
+int fomo_b200_server_submit(uint64_t server, uint64_t medium, const FomoHabc* habc, const FomoShot* shot,
+                            float* gather_out, uint64_t* ticket) {
+    auto s = find_server(server);
+    if (!s) return fail(FOMO_EINVAL, "unknown server handle %llu", (unsigned long long)server);
+    if (!ticket) return fail(FOMO_EINVAL, "ticket is NULL");
+    std::shared_ptr<Request> r;
+    {
+        std::lock_guard<std::mutex> lk(ctx().mu);
+        if (int rc = ensure_init()) return rc;
+        Medium* m = get<Medium>(medium);
+        if (!m) return fail(FOMO_EINVAL, "unknown medium handle %llu", (unsigned long long)medium);
+        if (int rc = make_request(m, habc, shot, gather_out, &r)) return rc;
+        m->users.fetch_add(1);
+    }
+    if (int rc = s->submit(r, ticket)) {
+        r->med->users.fetch_sub(1);
+        return rc;
+    }
+    return FOMO_OK;
+}
+
+int fomo_b200_server_poll(uint64_t server, uint64_t ticket, int32_t* done) {
+    auto s = find_server(server);
+    if (!s) return fail(FOMO_EINVAL, "unknown server handle %llu", (unsigned long long)server);
+    if (!done) return fail(FOMO_EINVAL, "done is NULL");
+    return s->poll(ticket, done);
+}
+
+int fomo_b200_server_wait(uint64_t server, uint64_t ticket, double timeout_s, FomoRequestStats* stats) {
+    auto s = find_server(server);
+    if (!s) return fail(FOMO_EINVAL, "unknown server handle %llu", (unsigned long long)server);
+    return s->wait(ticket, timeout_s, stats);
+}
+
+int fomo_b200_server_cancel(uint64_t server, uint64_t ticket) {
+    auto s = find_server(server);
+    if (!s) return fail(FOMO_EINVAL, "unknown server handle %llu", (unsigned long long)server);
+    return s->cancel(ticket);
+}
+
+int fomo_b200_server_stats(uint64_t server, FomoServerStats* stats) {
+    auto s = find_server(server);
+    if (!s) return fail(FOMO_EINVAL, "unknown server handle %llu", (unsigned long long)server);
+    if (!stats) return fail(FOMO_EINVAL, "stats is NULL");
+    s->get_stats(stats);
+    return FOMO_OK;
+}
+
+int fomo_b200_server_destroy(uint64_t server) {
+    std::shared_ptr<Server> s;
+    {
+        auto& T = servers();
+        std::lock_guard<std::mutex> lk(T.mu);
+        auto it = T.servers.find(server);
+        if (it == T.servers.end()) return fail(FOMO_EINVAL, "unknown server handle %llu", (unsigned long long)server);
+        s = it->second;
+        T.servers.erase(it);
+    }
+    s->shutdown();
+    return FOMO_OK;
+}
+
+int fomo_b200_run_batch(uint64_t medium, const FomoHabc* habc, const FomoShot* shots, int32_t n_shots,
+                        float* const* gathers_out, FomoRunStats* stats) {
+    if (n_shots < 0 || (n_shots > 0 && (!shots || !gathers_out))) return fail(FOMO_EINVAL, "bad shot arrays");
+    {
+        std::lock_guard<std::mutex> lk(ctx().mu);
+        if (int rc = ensure_init()) return rc;
+        if (!get<Medium>(medium)) return fail(FOMO_EINVAL, "unknown medium handle %llu", (unsigned long long)medium);
+        for (int s = 0; s < n_shots; ++s)
+            if (shots[s].dtx != shots[0].dtx || shots[s].dtz != shots[0].dtz)
+                return fail(FOMO_EINVAL, "shot %d has dtx/dtz different from shot 0's", s);
+    }
+    uint64_t h = 0;
+    FomoServerConfig cfg{};
+    if (int rc = fomo_b200_server_create(&cfg, &h)) return rc;
+    auto srv = find_server(h);
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0, srv->stream());
+    std::vector<uint64_t> tickets;
+    int rc = FOMO_OK;
+    for (int s = 0; s < n_shots && rc == FOMO_OK; ++s) {
+        uint64_t t = 0;
+        rc = fomo_b200_server_submit(h, medium, habc, &shots[s], gathers_out[s], &t);
+        if (rc == FOMO_OK) tickets.push_back(t);
+    }
+    std::string msg = rc ? g_err : std::string();
+    int64_t steps = 0;
+    for (uint64_t t : tickets) {
+        FomoRequestStats rs;
+        std::memset(&rs, 0, sizeof(rs));
+        const int w = fomo_b200_server_wait(h, t, -1.0, &rs);
+        if (w && rc == FOMO_OK) {
+            rc = w;
+            msg = g_err;
+        }
+        steps += rs.steps;
+    }
+    cudaEventRecord(e1, srv->stream());
+    cudaEventSynchronize(e1);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    FomoServerStats ss;
+    srv->get_stats(&ss);
+    srv.reset();
+    fomo_b200_server_destroy(h);
+    if (stats) {
+        stats->device_ms = ms;
+        stats->steps = steps;
+        stats->kernel_launches = ss.kernel_launches;
+        stats->h2d_bytes = ss.h2d_bytes;
+        stats->d2h_bytes = ss.d2h_bytes;
+    }
+    if (rc) g_err = msg;
+    return rc;
+}
+
+}  // extern "C"

@@ -38,6 +38,9 @@ namespace fomo {
 constexpr int kTX = 64, kTZ = 16, kThreads = 128;
 constexpr int kCG = kTX / 4;   // float4 column groups of a tile row
 constexpr int kBandW = 16;
+
+// Band blocks of a launch over a grid nx cells wide.
+__host__ __device__ constexpr int band_block_count(int nx) { return (nx + kBandW - 1) / kBandW; }
 constexpr int kEdgeX = 4, kEdgeZ = 2;  // margin of stencil values around an edge tile
 
 template <int M>

@@ -536,9 +536,21 @@ def create_source(M: Medium, shot: ShotConfig, wavelet) -> Source:
 def run_shots(b: B200Backend, W: Wavefield, M: Medium, H: HABCConfig, a, rec_template: Receivers,
               shot_config: MultiShotConfig, params: SimParams,
               on_shot_complete: Optional[Callable] = None, on_step: Optional[Callable] = None,
-              progress: bool = False, step_chunk: int = 1) -> List[ShotResult]:
+              progress: bool = False, step_chunk: int = 1, batched: bool = False) -> List[ShotResult]:
     """run_shots! (shot_manager.jl:145-180): the shots in order, one after
-    another, each with a fresh gather."""
+    another, each with a fresh gather.
+
+    batched=True runs all shots side by side instead (fomo_b200_run_batch:
+    every time-step launch covers every shot in flight); the gathers are the
+    same bit for bit, and `W` is not used.  on_step needs the sequential loop."""
+    if batched:
+        if on_step is not None:
+            raise ValueError("on_step needs the sequential loop (batched=False)")
+        results = run_batch(b, M, H, a, rec_template, shot_config, params)
+        if on_shot_complete is not None:
+            for r in results:
+                on_shot_complete(r)
+        return results
     results = []
     for shot in shot_config.shots:
         src = create_source(M, shot, shot_config.wavelet)
@@ -550,6 +562,32 @@ def run_shots(b: B200Backend, W: Wavefield, M: Medium, H: HABCConfig, a, rec_tem
         if on_shot_complete is not None:
             on_shot_complete(r)
     return results
+
+
+def run_batch(b: B200Backend, M: Medium, H: HABCConfig, a, rec_template: Receivers,
+              shot_config: MultiShotConfig, params: SimParams) -> List[ShotResult]:
+    """The shots of `shot_config` on one medium, run side by side
+    (fomo_b200_run_batch).  Returns one ShotResult per shot, in order; the
+    first result's stats cover the whole batch."""
+    keep: list = []
+    hs = _ctypes_habc(H, keep)
+    n = len(shot_config.shots)
+    shots = (FomoShot * max(n, 1))()
+    gathers, srcs = [], []
+    for k, shot in enumerate(shot_config.shots):
+        src = create_source(M, shot, shot_config.wavelet)
+        srcs.append(src)
+        shots[k] = _ctypes_shot(a, params, src, rec_template, keep)
+        gathers.append(np.zeros((params.nt, len(rec_template.i)), dtype=f32, order="F"))
+    ptrs = (ctypes.c_void_p * max(n, 1))(*[g.ctypes.data if g.size else None for g in gathers])
+    st = FomoRunStats()
+    mh = M.upload()
+    call("fomo_b200_run_batch", mh, ctypes.byref(hs), shots, n, ptrs, ctypes.byref(st))
+    return [ShotResult(gathers[k], int(shot.shot_id), int(srcs[k].i), int(srcs[k].j),
+                       np.asarray(rec_template.i, dtype=np.int64).copy(),
+                       np.asarray(rec_template.j, dtype=np.int64).copy(),
+                       _stats_dict(st) if k == 0 else None)
+            for k, shot in enumerate(shot_config.shots)]
 
 
 # ---------------------------------------------------------------------------

@@ -239,6 +239,84 @@ int fomo_b200_run_shot_noalloc(int32_t nx, int32_t nz, int32_t M, int32_t pad,
                                const FomoShot* shot, float* gather_out,
                                void* stream);
 
+/* ---------------------------------------------------------------------- */
+/* Batched shots and the shot server                                       */
+/* ---------------------------------------------------------------------- */
+
+/* run_shots! (src/simulation/shot_manager.jl:145-180) with the shots run
+ * side by side instead of one after another: every time-step launch covers
+ * all shots in flight, shots of one medium share its tiles in L2, and the
+ * time loop runs as CUDA graphs of K steps.  Each shot's gather is the same
+ * as fomo_b200_run_shot's for that shot, bit for bit.  The shots share the
+ * medium and HABC; their sources, receivers, wavelets and nt may differ
+ * (M, dtx, dtz and the coefficients a as for fomo_b200_run_shot; dtx and dtz
+ * equal across the shots).  gathers_out[s] is shot s's host gather
+ * (nt_s * n_rec_s floats).  Shots are admitted while their wavefields fit in
+ * 90% of free device memory, so any number of shots may be passed.  The call
+ * blocks until every gather is on the host.  stats (may be NULL) covers the
+ * whole batch: summed steps, device time, launches and bytes moved. */
+int fomo_b200_run_batch(uint64_t medium, const FomoHabc* habc, const FomoShot* shots,
+                        int32_t n_shots, float* const* gathers_out, FomoRunStats* stats);
+
+/* The shot server: a request loop (no reference counterpart; it serves
+ * run_shot! requests as they arrive).  A worker thread admits queued shots
+ * in arrival order while their device memory (two wavefield copies, HABC
+ * tables, receivers, wavelet, gather, and the buoyancy of a medium not yet
+ * resident) fits the HBM budget and the shot limit, and runs every admitted
+ * shot in the same launches, K steps at a time.  A shot joins the running
+ * batch at the next K-step boundary and leaves it when its nt steps are
+ * done; then its gather is copied back and its memory freed.  Shots overlap
+ * on the device whatever their media, orders and nt, and each result equals
+ * fomo_b200_run_shot's bit for bit. */
+typedef struct {
+    uint64_t hbm_budget_bytes;  /* device bytes for shots; 0 = 90% of free memory   */
+    int32_t max_shots;          /* shots on the device at once; 0 = budget only      */
+    int32_t steps_per_launch;   /* K; 0 = autotuned per (grid, order, batch size),   */
+                                /* 1 = one launch per kernel per step, no graphs     */
+} FomoServerConfig;
+
+typedef struct {
+    double queue_ms;            /* submit -> admitted                                */
+    double run_ms;              /* admitted -> gather on the host                    */
+    double latency_ms;          /* submit -> gather on the host                      */
+    int32_t steps;              /* time steps run (nt)                               */
+    int32_t batch_peak;         /* most shots on the device while this one ran       */
+} FomoRequestStats;
+
+typedef struct {
+    int64_t submitted, completed, failed, cancelled;
+    int64_t batch_steps;        /* time steps of the batch loop                      */
+    int64_t kernel_launches;    /* kernels run (graph replays count their kernels)   */
+    int64_t graph_replays;
+    int64_t h2d_bytes, d2h_bytes;
+    int32_t peak_shots;         /* most shots on the device at once                  */
+    int32_t steps_per_launch;   /* K of the last chunk                               */
+    uint64_t peak_bytes;        /* most budgeted device bytes held at once           */
+} FomoServerStats;
+
+int fomo_b200_server_create(const FomoServerConfig* config, uint64_t* server);
+/* Queues one shot (thread-safe, any host thread).  medium must stay alive
+ * until the request completes (fomo_b200_medium_destroy refuses a medium in
+ * use).  gather_out (host, nt*n_rec floats) is written by the server and
+ * must stay valid until wait reports the request done.  A shot that cannot
+ * fit the budget even alone fails here with FOMO_ENOMEM. */
+int fomo_b200_server_submit(uint64_t server, uint64_t medium, const FomoHabc* habc,
+                            const FomoShot* shot, float* gather_out, uint64_t* ticket);
+/* *done = 1 once the request has finished (then the return value is its
+ * status), 0 while it is queued or running. */
+int fomo_b200_server_poll(uint64_t server, uint64_t ticket, int32_t* done);
+/* Waits up to timeout_s seconds (< 0: no limit).  Returns the request's
+ * status and releases the ticket, or FOMO_ENOTREADY on timeout (the ticket
+ * stays valid).  stats may be NULL. */
+int fomo_b200_server_wait(uint64_t server, uint64_t ticket, double timeout_s,
+                          FomoRequestStats* stats);
+/* Cancels a request that is still queued (its wait returns FOMO_ECANCELLED);
+ * a running request is not interrupted and FOMO_EINVAL is returned. */
+int fomo_b200_server_cancel(uint64_t server, uint64_t ticket);
+int fomo_b200_server_stats(uint64_t server, FomoServerStats* stats);
+/* Cancels queued requests, lets running ones finish, stops the worker. */
+int fomo_b200_server_destroy(uint64_t server);
+
 #ifdef __cplusplus
 }
 #endif

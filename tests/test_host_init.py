@@ -97,3 +97,14 @@ def test_backend_names():
         F.backend("cpu")
     with pytest.raises(ValueError, match="Unknown backend"):
         F.backend(":cuda")
+
+
+def test_percentile_nearest_rank():
+    from fomo_julia_b200.serving import percentile
+    v = list(range(1, 101))
+    assert percentile(v, 50) == 50
+    assert percentile(v, 99) == 99
+    assert percentile(v, 100) == 100
+    assert percentile([7.0], 99) == 7.0
+    with pytest.raises(ValueError):
+        percentile([], 50)

@@ -100,6 +100,7 @@ struct Shot : Object {
     int nt = 0, src_i = 0, src_j = 0, n_rec = 0, rec_kind = 0;
     std::vector<float> wavelet;     // host copy: one sample per step
     float* d_tabs = nullptr;        // 3 x (nbc+2)
+    float* d_band = nullptr;        // band scratch: 3 planes of nbc rows x pitch
     int* d_rec = nullptr;           // n_rec linear offsets
     float* d_gather = nullptr;      // nt x n_rec
     int k_done = 0, recorded = 0;
@@ -107,6 +108,7 @@ struct Shot : Object {
     int64_t launches = 0, h2d = 0, d2h = 0;
     ~Shot() override {
         if (d_tabs) cudaFree(d_tabs);
+        if (d_band) cudaFree(d_band);
         if (d_rec) cudaFree(d_rec);
         if (d_gather) cudaFree(d_gather);
     }
@@ -145,6 +147,17 @@ uint64_t put(std::unique_ptr<Object> o) {
 
 int ensure_init() {
     if (!ctx().inited) return fail(FOMO_ENOINIT, "fomo_b200_init has not been called");
+    return FOMO_OK;
+}
+
+// The HABC band must fit the grid, and the free-surface rows (pad-5..pad,
+// 0-based) must lie above the bottom band and the row above it.
+int check_band(int nx, int nz, int pad, int fs, int nbc) {
+    if (nbc < 1 || 2 * nbc + 3 > nx || 2 * nbc + 2 > nz)
+        return fail(FOMO_EINVAL, "nbc=%d does not fit the %dx%d grid", nbc, nx, nz);
+    if (nbc + 2 > fomo::kMaxBandTab) return fail(FOMO_EINVAL, "nbc=%d above the supported %d", nbc, fomo::kMaxBandTab - 2);
+    if (fs && pad >= nz - nbc - 2)
+        return fail(FOMO_EINVAL, "free-surface rows reach the bottom HABC band (pad=%d, nbc=%d, nz=%d)", pad, nbc, nz);
     return FOMO_OK;
 }
 
@@ -248,7 +261,7 @@ Launch launch_shape(int nx, int nz, int nbc, bool iso) {
     L.tiles_z = (nz + fomo::kTZ - 1) / fomo::kTZ;
     L.x_last = std::max(0, (nx + 3) / 4 * 4 - fomo::kTX);  // last tile ends at the grid's right edge
     L.n_tile = L.tiles_x * L.tiles_z;
-    L.n_band = fomo::band_block_count(nx);
+    L.n_band = fomo::band_warp_count(nx);
     L.smem_v = fomo::tiled_smem_bytes<M>(true, nbc, iso);
     L.smem_s = fomo::tiled_smem_bytes<M>(false, nbc, iso);
     return L;
@@ -289,7 +302,7 @@ void fill_common(fomo::StepParams& P, const Medium& m, const Shot& s) {
 // Per-launch event pairs, filled only by fomo_b200_shot_profile.
 struct Profile {
     std::vector<cudaEvent_t> ev;      // 2 per launch
-    std::vector<int> kind;            // 0 velocity, 1 stress
+    std::vector<int> kind;            // 0 velocity, 1 stress, 2 band (velocity), 3 band (stress)
     int add(cudaStream_t st, int k) {
         cudaEvent_t a, b;
         if (cudaEventCreate(&a) != cudaSuccess || cudaEventCreate(&b) != cudaSuccess) return -1;
@@ -335,7 +348,7 @@ int run_steps_M(Shot& s, Medium& m, Wavefield& w, int n_steps, Profile* prof) {
     buoyancy_ptrs(m, T.b);
     T.iso = iso ? 1 : 0;
     T.status = C.d_status;
-    T.n_band_blocks = L.n_band;
+    T.band_pre = s.d_band;
     T.n_tile_blocks = L.n_tile;
     T.tiles_x = L.tiles_x;
     T.x_last = L.x_last;
@@ -352,7 +365,7 @@ int run_steps_M(Shot& s, Medium& m, Wavefield& w, int n_steps, Profile* prof) {
         P.out[fomo::VX] = w.field(b, fomo::VX);
         P.out[fomo::VZ] = w.field(b, fomo::VZ);
         P.rec_k = (k >= 2 && s.n_rec > 0) ? k - 1 : 0;
-        const int vblocks = L.n_band + L.n_tile + (P.rec_k ? rec_blocks : 0);
+        const int vblocks = L.n_tile + (P.rec_k ? rec_blocks : 0);
         if (prof && prof->add(C.stream, 0)) return fail(FOMO_ECUDA, "profiling event failed");
         fomo::VelMaps vm;
         vm.xx = w.maps[a][fomo::TXX];
@@ -365,6 +378,9 @@ int run_steps_M(Shot& s, Medium& m, Wavefield& w, int n_steps, Profile* prof) {
         vm.b2 = m.buoy_maps[2];
         vm.b3 = m.buoy_maps[3];
         fomo::velocity_kernel<M><<<vblocks, fomo::kThreads, L.smem_v, C.stream>>>(P, T, vm);
+        if (prof && prof->end(C.stream)) return fail(FOMO_ECUDA, "profiling event failed");
+        if (prof && prof->add(C.stream, 2)) return fail(FOMO_ECUDA, "profiling event failed");
+        fomo::band_kernel<true><<<L.n_band, 32, 0, C.stream>>>(P, T);
         if (prof && prof->end(C.stream)) return fail(FOMO_ECUDA, "profiling event failed");
         // stress: reads v(b) (new), tau(a); writes tau(b)
         P.in[fomo::VX] = w.field(b, fomo::VX);
@@ -382,9 +398,12 @@ int run_steps_M(Shot& s, Medium& m, Wavefield& w, int n_steps, Profile* prof) {
         sm.lam = m.mod_maps[0];
         sm.mu = m.mod_maps[1];
         sm.mxz = m.mod_maps[2];
-        fomo::stress_kernel<M><<<L.n_band + L.n_tile, fomo::kThreads, L.smem_s, C.stream>>>(P, T, sm);
+        fomo::stress_kernel<M><<<L.n_tile, fomo::kThreads, L.smem_s, C.stream>>>(P, T, sm);
         if (prof && prof->end(C.stream)) return fail(FOMO_ECUDA, "profiling event failed");
-        s.launches += 2;
+        if (prof && prof->add(C.stream, 3)) return fail(FOMO_ECUDA, "profiling event failed");
+        fomo::band_kernel<false><<<L.n_band, 32, 0, C.stream>>>(P, T);
+        if (prof && prof->end(C.stream)) return fail(FOMO_ECUDA, "profiling event failed");
+        s.launches += 4;
         w.cur = b;
         if (k >= 2) s.recorded = k - 1;
         s.k_done = k;
@@ -685,8 +704,7 @@ int fomo_b200_shot_begin(uint64_t medium, uint64_t wavefield, const FomoHabc* ha
     if (!shot->a) return fail(FOMO_EINVAL, "FD coefficients are NULL");
     if (shot->nt < 0) return fail(FOMO_EINVAL, "nt=%d < 0", shot->nt);
     const int nbc = habc->nbc;
-    if (nbc < 1 || 2 * nbc + 3 > m->nx || 2 * nbc + 2 > m->nz)
-        return fail(FOMO_EINVAL, "nbc=%d does not fit the %dx%d grid", nbc, m->nx, m->nz);
+    if (int rc = check_band(m->nx, m->nz, m->pad, m->fs, nbc)) return rc;
     if (!habc->w_vx || !habc->w_vz || !habc->w_tau) return fail(FOMO_EINVAL, "HABC weight tables are NULL");
     if (shot->src_i < 1 || shot->src_i > m->nx || shot->src_j < 1 || shot->src_j > m->nz)
         return fail(FOMO_EINVAL, "source (%d, %d) outside the %dx%d grid", shot->src_i, shot->src_j, m->nx, m->nz);
@@ -723,6 +741,7 @@ int fomo_b200_shot_begin(uint64_t medium, uint64_t wavefield, const FomoHabc* ha
     s->rec_kind = shot->rec_kind;
     const size_t tab_n = (size_t)nbc + 2;
     cudaError_t e = cudaMalloc(&s->d_tabs, 3 * tab_n * sizeof(float));
+    if (e == cudaSuccess) e = cudaMalloc(&s->d_band, 3 * (size_t)nbc * m->pitch * sizeof(float));
     if (e == cudaSuccess && s->n_rec) e = cudaMalloc(&s->d_rec, s->n_rec * sizeof(int));
     if (e == cudaSuccess && s->n_rec && s->nt)
         e = cudaMalloc(&s->d_gather, (size_t)s->nt * s->n_rec * sizeof(float));
@@ -785,24 +804,26 @@ int fomo_b200_shot_profile(uint64_t shot_handle, int32_t n_steps, FomoKernelTime
     if (int rc = ensure_init()) return rc;
     Shot* s = get<Shot>(shot_handle);
     if (!s) return fail(FOMO_EINVAL, "unknown shot handle %llu", (unsigned long long)shot_handle);
-    if (n_steps < 0 || n_steps > 100000 || !out || !n_kinds || max_kinds < 2)
-        return fail(FOMO_EINVAL, "bad profile arguments");
+    if (n_steps < 0 || n_steps > 100000 || !out || !n_kinds || max_kinds < 4)
+        return fail(FOMO_EINVAL, "bad profile arguments (max_kinds must be >= 4)");
     Medium* m = get<Medium>(s->medium);
     if (!m) return fail(FOMO_EINVAL, "shot refers to a destroyed medium");
     Profile prof;
     if (int rc = run_steps(*s, n_steps, &prof)) return rc;
     CUDA_TRY(cudaStreamSynchronize(ctx().stream));
-    // Algorithmic bytes of one launch over the nx*nz cells: velocity reads
-    // vx, vz, txx, tzz, txz, rho_vx, rho_vz and writes vx, vz (36 B/cell);
-    // stress reads vx, vz, txx, tzz, txz, lam, mu_txx, mu_txz and writes
-    // txx, tzz, txz (44 B/cell).
-    const double cells = (double)m->nx * m->nz;
-    const char* names[2] = {"velocity", "stress"};
-    const double bpc[2] = {36.0, 44.0};
-    for (int k = 0; k < 2; ++k) {
+    // Algorithmic bytes of one launch.  Tile launches, over the nx*nz cells:
+    // velocity reads vx, vz, txx, tzz, txz, rho_vx, rho_vz and writes vx, vz
+    // (36 B/cell); stress reads vx, vz, txx, tzz, txz, lam, mu_txx, mu_txz
+    // and writes txx, tzz, txz (44 B/cell).  Band passes, over the nbc*nx
+    // band cells: read the stencil value and the step-start value of each
+    // output field and write its final value (24 B/cell velocity, 36 stress).
+    const double cells = (double)m->nx * m->nz, band = (double)s->nbc * m->nx;
+    const char* names[4] = {"velocity", "stress", "band_velocity", "band_stress"};
+    const double bytes[4] = {36.0 * cells, 44.0 * cells, 24.0 * band, 36.0 * band};
+    for (int k = 0; k < 4; ++k) {
         std::memset(&out[k], 0, sizeof(FomoKernelTime));
         std::snprintf(out[k].name, sizeof(out[k].name), "%s", names[k]);
-        out[k].bytes_per_launch = bpc[k] * cells;
+        out[k].bytes_per_launch = bytes[k];
     }
     for (size_t i = 0; i < prof.kind.size(); ++i) {
         float ms = 0;
@@ -810,7 +831,7 @@ int fomo_b200_shot_profile(uint64_t shot_handle, int32_t n_steps, FomoKernelTime
         out[prof.kind[i]].launches += 1;
         out[prof.kind[i]].total_ms += ms;
     }
-    *n_kinds = 2;
+    *n_kinds = 4;
     return FOMO_OK;
 }
 
@@ -901,7 +922,6 @@ int noalloc_loop(const fomo::StepParams& P0, fomo::TiledArgs T, float* fields, i
         CUDA_TRY(cudaFuncSetAttribute(fomo::velocity_kernel<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.smem_v));
     if (L.smem_s > 48 * 1024)
         CUDA_TRY(cudaFuncSetAttribute(fomo::stress_kernel<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.smem_s));
-    T.n_band_blocks = L.n_band;
     T.n_tile_blocks = L.n_tile;
     T.tiles_x = L.tiles_x;
     T.x_last = L.x_last;
@@ -925,7 +945,8 @@ int noalloc_loop(const fomo::StepParams& P0, fomo::TiledArgs T, float* fields, i
         vm.b1 = bm[1];
         vm.b2 = bm[2];
         vm.b3 = bm[3];
-        fomo::velocity_kernel<M><<<L.n_band + L.n_tile + (P.rec_k ? rec_blocks : 0), fomo::kThreads, L.smem_v, st>>>(P, T, vm);
+        fomo::velocity_kernel<M><<<L.n_tile + (P.rec_k ? rec_blocks : 0), fomo::kThreads, L.smem_v, st>>>(P, T, vm);
+        fomo::band_kernel<true><<<L.n_band, 32, 0, st>>>(P, T);
         P.in[fomo::VX] = field(b, fomo::VX);
         P.in[fomo::VZ] = field(b, fomo::VZ);
         for (int q = 2; q < 5; ++q) P.out[q] = field(b, q);
@@ -940,7 +961,8 @@ int noalloc_loop(const fomo::StepParams& P0, fomo::TiledArgs T, float* fields, i
         sm.lam = mod[0];
         sm.mu = mod[1];
         sm.mxz = mod[2];
-        fomo::stress_kernel<M><<<L.n_band + L.n_tile, fomo::kThreads, L.smem_s, st>>>(P, T, sm);
+        fomo::stress_kernel<M><<<L.n_tile, fomo::kThreads, L.smem_s, st>>>(P, T, sm);
+        fomo::band_kernel<false><<<L.n_band, 32, 0, st>>>(P, T);
         cur = b;
     }
     if (n_rec > 0 && nt > 0) {  // receivers of the last step
@@ -973,7 +995,7 @@ extern "C" int fomo_b200_run_shot_noalloc(int32_t nx, int32_t nz, int32_t M, int
     if (shot->M != M || !shot->a) return fail(FOMO_EINVAL, "shot M=%d differs from medium M=%d or no coefficients", shot->M, M);
     if (shot->nt < 0 || shot->n_wavelet < 0 || (shot->n_wavelet > 0 && !shot->wavelet)) return fail(FOMO_EINVAL, "bad nt or wavelet");
     const int nbc = habc->nbc;
-    if (nbc < 1 || 2 * nbc + 3 > nx || 2 * nbc + 2 > nz) return fail(FOMO_EINVAL, "nbc=%d does not fit the %dx%d grid", nbc, nx, nz);
+    if (int rc = check_band(nx, nz, pad, free_surface ? 1 : 0, nbc)) return rc;
     if (!habc->w_vx || !habc->w_vz || !habc->w_tau) return fail(FOMO_EINVAL, "HABC weight tables are NULL");
     if (shot->src_i < 1 || shot->src_i > nx || shot->src_j < 1 || shot->src_j > nz)
         return fail(FOMO_EINVAL, "source (%d, %d) outside the %dx%d grid", shot->src_i, shot->src_j, nx, nz);
@@ -987,13 +1009,14 @@ extern "C" int fomo_b200_run_shot_noalloc(int32_t nx, int32_t nz, int32_t M, int
             return fail(FOMO_EINVAL, "receiver %d at (%d, %d) outside the %dx%d grid", r + 1, i, j, nx, nz);
         cells[r] = (i - 1) + (j - 1) * pitch;
     }
-    // Carve the scratch: status | tables | receiver offsets | buoyancy | wavefield.
+    // Carve the scratch: status | tables | receiver offsets | buoyancy | band | wavefield.
     const bool iso = shot->dtx == shot->dtz;
     const size_t plane = (size_t)pitch * nz * sizeof(float);
     const size_t off_tab = 256;
     const size_t off_rec = off_tab + align256(3 * (size_t)(nbc + 2) * sizeof(float));
     const size_t off_buo = off_rec + align256((size_t)shot->n_rec * sizeof(int));
-    const size_t off_wf = off_buo + align256((iso ? 2 : 4) * plane);
+    const size_t off_band = off_buo + align256((iso ? 2 : 4) * plane);
+    const size_t off_wf = off_band + align256(3 * (size_t)nbc * pitch * sizeof(float));
     const size_t need = off_wf + 10 * plane;
     if (need > kNoAllocScratchBytes)
         return fail(FOMO_EINVAL, "shot needs %zu bytes of scratch, more than the %zu-byte static array of "
@@ -1007,6 +1030,7 @@ extern "C" int fomo_b200_run_shot_noalloc(int32_t nx, int32_t nz, int32_t M, int
     int* d_rec = reinterpret_cast<int*>(base + off_rec);
     float* d_buo = reinterpret_cast<float*>(base + off_buo);
     float* d_fields = reinterpret_cast<float*>(base + off_wf);
+    float* d_band = reinterpret_cast<float*>(base + off_band);
     const size_t tab_n = (size_t)nbc + 2;
     CUDA_TRY(cudaMemsetAsync(d_status, 0, sizeof(int), st));
     CUDA_TRY(cudaMemsetAsync(d_fields, 0, 10 * plane, st));
@@ -1060,6 +1084,7 @@ extern "C" int fomo_b200_run_shot_noalloc(int32_t nx, int32_t nz, int32_t M, int
     T.b[3] = b3;
     T.iso = iso ? 1 : 0;
     T.status = d_status;
+    T.band_pre = d_band;
     const float* bp[4] = {b0, b1, b2, b3};
     int rc = FOMO_EINVAL;
     switch (M) {

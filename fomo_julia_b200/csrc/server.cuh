@@ -8,9 +8,10 @@
 //   admit   queued requests, in arrival order, while their device bytes fit
 //           the HBM budget (and the shot limit); allocate and upload each
 //           shot, starting it at the next batch step;
-//   run     K batch steps: per FD order, one velocity and one stress launch
-//           over every shot in flight (step_batch.cuh), then the step-counter
-//           advance; K steps are one CUDA graph replay once captured;
+//   run     K batch steps: per FD order, a velocity tile launch and its band
+//           pass, a stress tile launch and its band pass, each over every
+//           shot in flight (step_batch.cuh), then the step-counter advance;
+//           K steps are one CUDA graph replay once captured;
 //   retire  shots whose nt steps are done: record the last step's receivers,
 //           copy the gather to pinned memory, free the shot's memory (stream
 //           ordered), and hand the gather to the caller once its copy lands.
@@ -103,7 +104,7 @@ struct Request {
     float* d_gather = nullptr;
     Resident* res = nullptr;
     int start = 0;           // batch step of the shot's step 1
-    size_t tabs_off = 0, cells_off = 0, wav_off = 0, gather_off = 0;
+    size_t band_off = 0, tabs_off = 0, cells_off = 0, wav_off = 0, gather_off = 0;
     fomo::ShotDev dev;       // host image of the shot's table entry
     void* staging = nullptr; // pinned: gather + status word
     cudaEvent_t done_ev = nullptr;
@@ -186,11 +187,11 @@ void launch_batch(int M, bool vel, const fomo::BatchArgs& B, int grid, size_t sm
     }
 }
 
-// The shots of one FD order in flight: one velocity and one stress launch.
+// The shots of one FD order in flight: their launches of one step.
 struct LaunchSet {
     int M = 0;
     fomo::BatchArgs args{};
-    int grid_v = 0, grid_s = 0;
+    int grid_v = 0, grid_s = 0, grid_b = 0;  // velocity tiles + receivers, stress tiles, band passes
     size_t smem_v = 0, smem_s = 0;
 };
 
@@ -541,12 +542,15 @@ class Server {
         L.tiles_z = (m.nz + fomo::kTZ - 1) / fomo::kTZ;
         L.x_last = std::max(0, (m.nx + 3) / 4 * 4 - fomo::kTX);
         L.n_tile = L.tiles_x * L.tiles_z;
-        L.n_band = fomo::band_block_count(m.nx);
+        L.n_band = fomo::band_warp_count(m.nx);
         const bool iso = r.dtx == r.dtz;
         L.smem_v = batch_smem_any(r.M, true, r.nbc, iso);
         L.smem_s = batch_smem_any(r.M, false, r.nbc, iso);
         return L;
     }
+
+    // Bytes of a shot's band scratch (three planes of nbc rows).
+    static size_t band_bytes(const Request& r) { return 3 * (size_t)r.nbc * r.med->pitch * sizeof(float); }
 
     // Bytes of the pinned upload area of a shot.
     static size_t stage_bytes(const Request& r) {
@@ -563,7 +567,8 @@ class Server {
         r.res->refs += 1;
         const Medium& m = *r.med;
         const size_t plane = (size_t)m.pitch * m.nz * sizeof(float);
-        r.tabs_off = 10 * plane;
+        r.band_off = 10 * plane;
+        r.tabs_off = r.band_off + align_up(band_bytes(r), 256);
         r.cells_off = r.tabs_off + align_up(r.tabs.size() * 4, 256);
         r.wav_off = r.cells_off + align_up(r.cells.size() * 4, 256);
         r.gather_off = r.wav_off + align_up(std::max<size_t>(r.wavelet.size(), 1) * 4, 256);
@@ -625,7 +630,7 @@ class Server {
         for (int q = 0; q < 4; ++q) T.b[q] = r.res->b[q];
         T.iso = r.res->iso;
         T.status = d_status_;
-        T.n_band_blocks = L.n_band;
+        T.band_pre = reinterpret_cast<float*>(base + r.band_off);
         T.n_tile_blocks = L.n_tile;
         T.tiles_x = L.tiles_x;
         T.x_last = L.x_last;
@@ -696,8 +701,9 @@ class Server {
             S.args.n_groups = (int)p.groups.size();
             S.args.total_band = band;
             S.args.total_tile = tile;
-            S.grid_v = band + tile + rec;
-            S.grid_s = band + tile;
+            S.grid_v = tile + rec;
+            S.grid_s = tile;
+            S.grid_b = band;
             p.shots_off = bytes;
             bytes += align_up(p.n * sizeof(fomo::ShotDev), 256);
             p.groups_off = bytes;
@@ -760,11 +766,13 @@ class Server {
     }
 
     // ------------------------------------------------------------ stepping
-    int launches_per_step() const { return 2 * (int)sets_.size() + 1; }
+    int launches_per_step() const { return 4 * (int)sets_.size() + 1; }
 
     void enqueue_step() {
         for (const LaunchSet& S : sets_) launch_batch(S.M, true, S.args, S.grid_v, S.smem_v, st_);
+        for (const LaunchSet& S : sets_) fomo::batch_band_kernel<true><<<S.grid_b, 32, 0, st_>>>(S.args);
         for (const LaunchSet& S : sets_) launch_batch(S.M, false, S.args, S.grid_s, S.smem_s, st_);
+        for (const LaunchSet& S : sets_) fomo::batch_band_kernel<false><<<S.grid_b, 32, 0, st_>>>(S.args);
         fomo::batch_advance_kernel<<<1, 1, 0, st_>>>(d_step_);
     }
 
@@ -1143,8 +1151,7 @@ int make_request(Medium* m, const FomoHabc* habc, const FomoShot* shot, float* g
     if (!shot->a) return fail(FOMO_EINVAL, "FD coefficients are NULL");
     if (shot->nt < 0) return fail(FOMO_EINVAL, "nt=%d < 0", shot->nt);
     const int nbc = habc->nbc;
-    if (nbc < 1 || 2 * nbc + 3 > m->nx || 2 * nbc + 2 > m->nz)
-        return fail(FOMO_EINVAL, "nbc=%d does not fit the %dx%d grid", nbc, m->nx, m->nz);
+    if (int rc = check_band(m->nx, m->nz, m->pad, m->fs, nbc)) return rc;
     if (!habc->w_vx || !habc->w_vz || !habc->w_tau) return fail(FOMO_EINVAL, "HABC weight tables are NULL");
     if (shot->src_i < 1 || shot->src_i > m->nx || shot->src_j < 1 || shot->src_j > m->nz)
         return fail(FOMO_EINVAL, "source (%d, %d) outside the %dx%d grid", shot->src_i, shot->src_j, m->nx, m->nz);
@@ -1189,7 +1196,7 @@ int make_request(Medium* m, const FomoHabc* habc, const FomoShot* shot, float* g
     }
     r->gather_out = gather_out;
     const size_t plane = (size_t)m->pitch * m->nz * sizeof(float);
-    r->bytes = 10 * plane + align_up(r->tabs.size() * 4, 256) + align_up(r->cells.size() * 4, 256) +
+    r->bytes = 10 * plane + align_up(3 * (size_t)nbc * m->pitch * sizeof(float), 256) + align_up(r->tabs.size() * 4, 256) + align_up(r->cells.size() * 4, 256) +
                align_up(std::max<size_t>(r->wavelet.size(), 1) * 4, 256) +
                align_up((size_t)r->nt * r->n_rec * 4, 256);
     r->buoy_bytes = (iso ? 2 : 4) * plane;

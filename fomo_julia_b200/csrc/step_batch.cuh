@@ -7,19 +7,19 @@
 // can be captured once into a CUDA graph and replayed.
 //
 // Shots are grouped by medium (same nx, nz, hence the same block counts).
-// One launch holds, for every shot s whose local step ks = k - start_s + 1
+// A tile launch holds, for every shot s whose local step ks = k - start_s + 1
 // lies in 1..nt_s (k = batch step):
-//   band blocks   all groups, then
 //   tile blocks   all groups, then
-//   receivers     (velocity launch only) the receivers of step ks-1.
-// Inside a group, band and tile blocks are interleaved tile-major
+//   receivers     (velocity launch only) the receivers of step ks-1;
+// the band launch that follows it holds the band-pass warps of every group.
+// Inside a group, tile and band blocks are interleaved tile-major
 // (block = local * n + shot), so the n shots' copies of one tile run side by
 // side and the medium tile is read from HBM once and from L2 by the others.
 // A block whose shot is outside its step range returns at once; that is how
 // shots join and leave a running batch at step boundaries.
 //
-// Every block runs the single-shot code (band_block, edge_tile, fast_vel,
-// fast_str, record_block) on its shot's parameters, so a batched shot's
+// Every block runs the single-shot code (edge_tile, fast_vel, fast_str,
+// record_block, band_march) on its shot's parameters, so a batched shot's
 // results are bit-identical to the same shot run alone.
 #pragma once
 
@@ -44,8 +44,8 @@ struct alignas(64) ShotDev {
 // Shots first..first+n-1 of the table share a medium.
 struct GroupDev {
     int first, n;
-    int n_band, n_tile;     // blocks per shot
-    int band_off, tile_off; // first band / tile block of the group in a launch
+    int n_band, n_tile;     // band-pass and tile blocks per shot
+    int band_off, tile_off; // first band / tile block of the group in its launch
 };
 
 struct BatchArgs {
@@ -58,7 +58,7 @@ struct BatchArgs {
 };
 
 struct BatchItem {
-    int role;   // 0 band, 1 tile, 2 receivers, -1 none
+    int role;   // 0 band pass, 1 tile, 2 receivers, -1 none
     int shot, local;
 };
 
@@ -79,9 +79,9 @@ __device__ __forceinline__ BatchItem in_groups(const BatchArgs& B, int b) {
     return it;
 }
 
-__device__ __forceinline__ BatchItem decode(const BatchArgs& B, int bid, bool vel) {
-    if (bid < B.total_band) return in_groups<false>(B, bid);
-    bid -= B.total_band;
+// Block bid of a tile launch (band == false) or of a band launch.
+__device__ __forceinline__ BatchItem decode(const BatchArgs& B, int bid, bool vel, bool band) {
+    if (band) return in_groups<false>(B, bid);
     if (bid < B.total_tile) return in_groups<true>(B, bid);
     bid -= B.total_tile;
     BatchItem it{-1, 0, 0};
@@ -115,11 +115,11 @@ __device__ __forceinline__ void tensormap_acquire(const CUtensorMap* m) {
 
 // Thread 0 decodes the block; all threads copy the shot's parameters; thread 0
 // then sets the per-step fields.  Returns false for an idle block.
-template <bool VEL>
+template <bool VEL, bool BAND>
 __device__ __forceinline__ bool setup_block(const BatchArgs& B, BatchBlock& bb) {
     if (threadIdx.x == 0) {
         bb.ks = 0;
-        bb.it = decode(B, blockIdx.x, VEL);
+        bb.it = decode(B, blockIdx.x, VEL, BAND);
         if (bb.it.role >= 0) {
             const ShotDev& sd = B.shots[bb.it.shot];
             const int ks = *B.step - sd.start + 1;
@@ -174,12 +174,10 @@ template <int M>
 __global__ void __launch_bounds__(kThreads, 5) batch_velocity_kernel(const __grid_constant__ BatchArgs B) {
     extern __shared__ __align__(128) float smem[];
     __shared__ BatchBlock bb;
-    if (!setup_block<true>(B, bb)) return;
+    if (!setup_block<true, false>(B, bb)) return;
     const StepParams& P = bb.P;
     const TiledArgs& T = bb.T;
-    if (bb.it.role == 0) {
-        band_block<M, true>(P, T, bb.it.local, smem);
-    } else if (bb.it.role == 1) {
+    if (bb.it.role == 1) {
         const TileKind k = classify(P, T, bb.it.local);
         if (k.generic) edge_tile<M, true>(P, T, k.x0, k.z0, k.x_end, smem);
         else fast_vel<M>(P, T, B.shots[bb.it.shot].vmap[bb.a], k.x0, k.z0, k.x_end, k.band, k.rim, smem);
@@ -192,16 +190,25 @@ template <int M>
 __global__ void __launch_bounds__(kThreads, 5) batch_stress_kernel(const __grid_constant__ BatchArgs B) {
     extern __shared__ __align__(128) float smem[];
     __shared__ BatchBlock bb;
-    if (!setup_block<false>(B, bb)) return;
+    if (!setup_block<false, false>(B, bb)) return;
     const StepParams& P = bb.P;
     const TiledArgs& T = bb.T;
-    if (bb.it.role == 0) {
-        band_block<M, false>(P, T, bb.it.local, smem);
-    } else {
+    {
         const TileKind k = classify(P, T, bb.it.local);
         if (k.generic) edge_tile<M, false>(P, T, k.x0, k.z0, k.x_end, smem);
         else fast_str<M>(P, T, B.shots[bb.it.shot].smap[bb.a], k.x0, k.z0, k.x_end, k.band, k.rim, smem);
     }
+}
+
+// Band pass of every shot in flight (after the tile launch of the same half
+// step): one warp per (shot, strip, field).
+template <bool VEL>
+__global__ void __launch_bounds__(32) batch_band_kernel(const __grid_constant__ BatchArgs B) {
+    __shared__ __align__(16) float stage[kMarchStage];
+    __shared__ float stab[kMaxBandTab];
+    __shared__ BatchBlock bb;
+    if (!setup_block<VEL, true>(B, bb)) return;
+    band_march<VEL>(bb.P, bb.T, bb.it.local, stage, stab);
 }
 
 // Advances the batch step counter; launched once per step after the stress

@@ -6,12 +6,7 @@
 // function of read-only inputs and no ordering is needed inside a launch.
 // Block roles of one launch, in launch order:
 //
-//   [0, n_band)              bottom band: rows nz-nbc-1..nz-2 (bottom edge and
-//                            corners), kBandW columns per block; the HABC
-//                            recurrence along j runs down the band in shared
-//                            memory.  First in the grid so their serial part
-//                            overlaps the tiles.
-//   [n_band, +n_tiles)       64 x 16 cell tiles in raster order; the last tile
+//   [0, n_tiles)             64 x 16 cell tiles in raster order; the last tile
 //                            of a row is aligned to the right edge of the grid
 //                            so that the right HABC band and the two columns
 //                            its rules read lie in one tile, as the left band
@@ -27,6 +22,11 @@
 //         wider than a tile allows): stencil values of the tile plus a 4 x 2
 //         margin are computed into shared memory cell by cell, then the rules.
 //   [.., +record blocks)     receivers of step rec_k (velocity launch only).
+//
+// Rows nz-nbc-1 .. nz-2 (the bottom HABC band) are stored by the tiles
+// before their HABC, into a band scratch; a second launch per half step, the
+// band pass (band_kernel), runs the band's recurrence along j and writes the
+// final values.
 #pragma once
 
 #include <cuda.h>
@@ -37,10 +37,11 @@ namespace fomo {
 
 constexpr int kTX = 64, kTZ = 16, kThreads = 128;
 constexpr int kCG = kTX / 4;   // float4 column groups of a tile row
-constexpr int kBandW = 16;
+constexpr int kStripW = 28;     // columns a band-pass warp stores
+constexpr int kMarchRows = 16;  // band rows staged per chunk by the band pass
 
-// Band blocks of a launch over a grid nx cells wide.
-__host__ __device__ constexpr int band_block_count(int nx) { return (nx + kBandW - 1) / kBandW; }
+// Band-pass strips over a grid nx cells wide.
+__host__ __device__ constexpr int band_block_count(int nx) { return (nx + kStripW - 1) / kStripW; }
 constexpr int kEdgeX = 4, kEdgeZ = 2;  // margin of stencil values around an edge tile
 
 template <int M>
@@ -60,7 +61,8 @@ struct TiledArgs {
     const float* b[4];   // buoyancy dtx/rho_vx, dtz/rho_vx, dtx/rho_vz, dtz/rho_vz
     int iso;             // dtx == dtz: b[1] == b[0] and b[3] == b[2]
     int* status;         // first nonzero error code of the launch (0 = ok)
-    int n_band_blocks, n_tile_blocks, tiles_x;
+    float* band_pre;     // pre-HABC values of the bottom band rows (see band_pre_at)
+    int n_tile_blocks, tiles_x;
     int x_last;          // first column of the last tile of a row (a multiple of 4)
 };
 
@@ -149,10 +151,22 @@ __device__ __forceinline__ bool wait_tma(uint64_t* bar, const TiledArgs& T) {
     return false;
 }
 
-// Rows a tile stores: inside the grid and outside the bottom band (the band
-// blocks write whole band rows).
-__device__ __forceinline__ bool row_stored(const StepParams& P, int j) {
-    return j < P.nz && !(j >= P.nz - P.nbc - 1 && j <= P.nz - 2);
+// Rows a tile stores: every row of the grid.  Rows nz-nbc-1 .. nz-2 (the
+// bottom band) are stored before their HABC, into the band scratch, for the
+// band pass to finish.
+__device__ __forceinline__ bool row_stored(const StepParams& P, int j) { return j < P.nz; }
+
+// Band scratch: output field f (0, 1[, 2] of the half step) of band row
+// jb = j - (nz-nbc-1), as planes of nbc rows with the grid's row pitch.
+__device__ __forceinline__ float* band_pre_at(const StepParams& P, const TiledArgs& T, int f, int jb, int i) {
+    return T.band_pre + ((size_t)f * P.nbc + jb) * P.pitch + i;
+}
+
+// Where a tile stores output field f (pointer `out`) of cell (i, j).
+__device__ __forceinline__ float* store_at(const StepParams& P, const TiledArgs& T, float* out, int f, int i, int j) {
+    const int jb = j - (P.nz - P.nbc - 1);
+    if (jb >= 0 && jb < P.nbc) return band_pre_at(P, T, f, jb, i);
+    return out + cell(P, i, j);
 }
 
 __device__ __forceinline__ bool lr_band_cell(const StepParams& P, int i, int j) {
@@ -247,143 +261,6 @@ struct SmemPre {
     __device__ float operator()(int i, int j) const { return spre[(f * H + (j - za)) * W + (i - xa)]; }
 };
 
-// ---------------------------------------------------------------- bottom band
-// Rows nz-nbc-1 .. nz-2, columns 1 .. nx-2: the bottom edge and the two
-// bottom corners.  Stencil values of the block's columns (plus a 3-column
-// halo) and the row above the band are computed into shared memory; then one
-// thread per column marches down the rows.  In a row, the bottom edge,
-// bottom-left cells below nbc and bottom-right cells that are not chunk
-// starts read stencil values of row j and finals of row j-1 (phase A); the
-// last bottom-left column reads the bottom edge's final value at i+1 and a
-// bottom-right chunk start the final value at i-1 (phase B).
-template <int M, bool VEL>
-__device__ void band_block(const StepParams& P, const TiledArgs& T, int bblock, float* smem) {
-    constexpr int NF = VEL ? 2 : 3;
-    const int b = P.nbc, nx = P.nx, nz = P.nz;
-    const int R = b + 1;              // rows nz-b-2 .. nz-2
-    const int C = kBandW + 6;         // cols x0-3 .. x0+kBandW+2
-    const int CF = kBandW + 2;        // chain cols x0-1 .. x0+kBandW
-    const int x0 = bblock * kBandW;
-    const int j_top = nz - b - 2;
-    // [stencil inputs, later the step-start values][stencil values][two chain rows]
-    const int n_in = (VEL ? 3 : 2) * (C + 2 * M) * (R + 2 * M);
-    float* sin = smem;                                    // NF_in x (C+2M) x (R+2M)
-    float* Om = smem;                                     // NF x R x C, once sin is dead
-    float* Pm = smem + max(n_in, NF * R * C);             // NF x R x C
-    float* Fa = Pm + NF * R * C;                          // NF x CF
-    float* Fb = Fa + NF * CF;
-    const int fidx[3] = {VEL ? VX : TXX, VEL ? VZ : TZZ, TXZ};
-
-    load_region_inputs<M, VEL>(P, x0 - 3, j_top, C, R, sin);
-    __syncthreads();
-    compute_region_pre<M, VEL>(P, T, x0 - 3, j_top, C, R, sin, Pm);
-    __syncthreads();
-    for (int idx = threadIdx.x; idx < NF * R * C; idx += blockDim.x) {
-        const int f = idx / (R * C), r = idx - f * (R * C);
-        const int rr = r / C, c = r - rr * C;
-        const int i = x0 - 3 + c, j = j_top + rr;
-        const int q = VEL ? VX + f : TXX + f;
-        Om[idx] = (i >= 0 && i < nx) ? __ldg(in_field(P, q) + cell(P, i, j)) : 0.f;
-    }
-    __syncthreads();
-
-    const float* tabs[3] = {P.w_tab[VEL ? 0 : 2], P.w_tab[VEL ? 1 : 2], P.w_tab[2]};
-    auto PV = [&](int f, int i, int j) -> float { return Pm[(f * R + (j - j_top)) * C + (i - x0 + 3)]; };
-    auto OV = [&](int f, int i, int j) -> float { return Om[(f * R + (j - j_top)) * C + (i - x0 + 3)]; };
-    auto Wt = [&](int f, int i, int j) -> float { return habc_w(tabs[f], b, nx, nz, i, j); };
-    const int r0 = nx - b - 1;
-
-    // Row nz-b-2: values after the edge loops.
-    for (int cc = threadIdx.x; cc < CF; cc += blockDim.x) {
-        const int i = x0 - 1 + cc, j = j_top;
-#pragma unroll
-        for (int f = 0; f < NF; ++f) {
-            float val = 0.f;
-            if (i >= 0 && i < nx) {
-                val = PV(f, i, j);
-                if (i >= 1 && i <= b) {
-                    val = blend_edge(Wt(f, i, j), PV(f, i, j),
-                                     edge_sum(P.qx, P.qt_x, P.qxt, PV(f, i + 1, j), OV(f, i, j), OV(f, i + 1, j)));
-                } else if (i >= r0 && i <= nx - 2) {
-                    auto rplain = [&](int ii) {
-                        return blend_edge(Wt(f, ii, j), PV(f, ii, j),
-                                          edge_sum(P.qx, P.qt_x, P.qxt, PV(f, ii - 1, j), OV(f, ii, j), OV(f, ii - 1, j)));
-                    };
-                    if (i > r0 && right_chunk_start(nx, b, i)) {
-                        val = blend_edge(Wt(f, i, j), PV(f, i, j),
-                                         edge_sum(P.qx, P.qt_x, P.qxt, rplain(i - 1), OV(f, i, j), OV(f, i - 1, j)));
-                    } else {
-                        val = rplain(i);
-                    }
-                }
-            }
-            Fa[f * CF + cc] = val;
-        }
-    }
-    __syncthreads();
-
-    float* Fprev = Fa;
-    float* Fcur = Fb;
-    for (int j = j_top + 1; j <= nz - 2; ++j) {
-        for (int cc = threadIdx.x; cc < CF; cc += blockDim.x) {
-            const int i = x0 - 1 + cc;
-            if (i < 0 || i >= nx) continue;
-            const bool phase_b = (i == b) || (i >= r0 && i <= nx - 2 && right_chunk_start(nx, b, i));
-            if (phase_b && i >= 1 && i <= nx - 2) continue;
-#pragma unroll
-            for (int f = 0; f < NF; ++f) {
-                float val;
-                const float own = PV(f, i, j);
-                if (i == 0 || i == nx - 1) {
-                    val = own;
-                } else if (i <= b) {  // bottom-left corner
-                    const float sx = edge_sum(P.qx, P.qt_x, P.qxt, PV(f, i + 1, j), OV(f, i, j), OV(f, i + 1, j));
-                    const float sz = edge_sum(P.qz, P.qt_z, P.qxt, Fprev[f * CF + cc], OV(f, i, j), OV(f, i, j - 1));
-                    val = blend_corner(Wt(f, i, j), own, sx, sz);
-                } else if (i >= r0) {  // bottom-right corner
-                    const float sx = edge_sum(P.qx, P.qt_x, P.qxt, PV(f, i - 1, j), OV(f, i, j), OV(f, i - 1, j));
-                    const float sz = edge_sum(P.qz, P.qt_z, P.qxt, Fprev[f * CF + cc], OV(f, i, j), OV(f, i, j - 1));
-                    val = blend_corner(Wt(f, i, j), own, sx, sz);
-                } else {  // bottom edge
-                    val = blend_edge(Wt(f, i, j), own,
-                                     edge_sum(P.qz, P.qt_z, P.qxt, Fprev[f * CF + cc], OV(f, i, j), OV(f, i, j - 1)));
-                }
-                Fcur[f * CF + cc] = val;
-            }
-        }
-        __syncthreads();
-        for (int cc = threadIdx.x; cc < CF; cc += blockDim.x) {
-            const int i = x0 - 1 + cc;
-            if (i < 1 || i > nx - 2) continue;
-            const bool bl_last = (i == b);
-            const bool br_start = (i >= r0 && right_chunk_start(nx, b, i));
-            if (!bl_last && !br_start) continue;
-            if (bl_last && cc + 1 >= CF) continue;  // halo column: value unused
-            if (br_start && cc == 0) continue;      // halo column: value unused
-#pragma unroll
-            for (int f = 0; f < NF; ++f) {
-                const float own = PV(f, i, j);
-                const int ix = bl_last ? i + 1 : i - 1;
-                const float fx = Fcur[f * CF + (bl_last ? cc + 1 : cc - 1)];
-                const float sx = edge_sum(P.qx, P.qt_x, P.qxt, fx, OV(f, i, j), OV(f, ix, j));
-                const float sz = edge_sum(P.qz, P.qt_z, P.qxt, Fprev[f * CF + cc], OV(f, i, j), OV(f, i, j - 1));
-                Fcur[f * CF + cc] = blend_corner(Wt(f, i, j), own, sx, sz);
-            }
-        }
-        __syncthreads();
-        for (int cc = 1 + threadIdx.x; cc <= kBandW; cc += blockDim.x) {
-            const int i = x0 - 1 + cc;
-            if (i < 0 || i > nx - 1) continue;  // the whole row, rim columns included
-#pragma unroll
-            for (int f = 0; f < NF; ++f) P.out[fidx[f]][cell(P, i, j)] = Fcur[f * CF + cc];
-        }
-        float* t = Fprev;
-        Fprev = Fcur;
-        Fcur = t;
-        __syncthreads();
-    }
-}
-
 // ---------------------------------------------------------------- edge tiles
 template <int M, bool VEL>
 __device__ void edge_tile(const StepParams& P, const TiledArgs& T, int x0, int z0, int x_end, float* smem) {
@@ -399,7 +276,6 @@ __device__ void edge_tile(const StepParams& P, const TiledArgs& T, int x0, int z
         const int i = x0 + (idx % kTX), j = z0 + (idx / kTX);
         if (i >= P.nx || i >= x_end || !row_stored(P, j)) continue;
         const bool band = (i <= P.nbc) || (i >= P.nx - P.nbc - 1) || (!P.fs && j <= P.nbc);
-        const size_t c = cell(P, i, j);
         if (VEL) {
             float vx = SmemPre{spre, xa, za, G::RW, G::RH, 0}(i, j);
             float vz = SmemPre{spre, xa, za, G::RW, G::RH, 1}(i, j);
@@ -407,8 +283,8 @@ __device__ void edge_tile(const StepParams& P, const TiledArgs& T, int x0, int z
                 vx = HabcPoint<SmemPre>{P, SmemPre{spre, xa, za, G::RW, G::RH, 0}, P.in[VX], P.w_tab[0]}.final_value(i, j);
                 vz = HabcPoint<SmemPre>{P, SmemPre{spre, xa, za, G::RW, G::RH, 1}, P.in[VZ], P.w_tab[1]}.final_value(i, j);
             }
-            P.out[VX][c] = vx;
-            P.out[VZ][c] = vz;
+            *store_at(P, T, P.out[VX], 0, i, j) = vx;
+            *store_at(P, T, P.out[VZ], 1, i, j) = vz;
         } else {
             float v[3];
 #pragma unroll
@@ -417,9 +293,9 @@ __device__ void edge_tile(const StepParams& P, const TiledArgs& T, int x0, int z
                 v[f] = band ? HabcPoint<SmemPre>{P, pre, P.in[TXX + f], P.w_tab[2]}.final_value(i, j) : pre(i, j);
             }
             if (in_free_surface_rows(P, j)) v[1] = v[2] = 0.f;
-            P.out[TXX][c] = v[0];
-            P.out[TZZ][c] = v[1];
-            P.out[TXZ][c] = v[2];
+            *store_at(P, T, P.out[TXX], 0, i, j) = v[0];
+            *store_at(P, T, P.out[TZZ], 1, i, j) = v[1];
+            *store_at(P, T, P.out[TXZ], 2, i, j) = v[2];
         }
     }
 }
@@ -595,9 +471,8 @@ __device__ __forceinline__ void fast_vel(const StepParams& P, const TiledArgs& T
 #pragma unroll
         for (int rr = 0; rr < 2; ++rr)
             if (row_stored(P, zt + rr)) {
-                const size_t cc = cell(P, x, zt + rr);
-                stg4(P.out[VX] + cc, ox[rr]);
-                stg4(P.out[VZ] + cc, oz[rr]);
+                stg4(store_at(P, T, P.out[VX], 0, x, zt + rr), ox[rr]);
+                stg4(store_at(P, T, P.out[VZ], 1, x, zt + rr), oz[rr]);
             }
     }
 }
@@ -727,10 +602,9 @@ __device__ __forceinline__ void fast_str(const StepParams& P, const TiledArgs& T
                     ozz[rr] = make_float4(0.f, 0.f, 0.f, 0.f);
                     oxz[rr] = make_float4(0.f, 0.f, 0.f, 0.f);
                 }
-                const size_t cc = cell(P, x, zt + rr);
-                stg4(P.out[TXX] + cc, oxx[rr]);
-                stg4(P.out[TZZ] + cc, ozz[rr]);
-                stg4(P.out[TXZ] + cc, oxz[rr]);
+                stg4(store_at(P, T, P.out[TXX], 0, x, zt + rr), oxx[rr]);
+                stg4(store_at(P, T, P.out[TZZ], 1, x, zt + rr), ozz[rr]);
+                stg4(store_at(P, T, P.out[TXZ], 2, x, zt + rr), oxz[rr]);
             }
     }
 }
@@ -777,12 +651,7 @@ template <int M>
 __global__ void __launch_bounds__(kThreads, 5) velocity_kernel(const __grid_constant__ StepParams P, const __grid_constant__ TiledArgs T,
                                                             const __grid_constant__ VelMaps maps) {
     extern __shared__ __align__(128) float smem[];
-    int bid = blockIdx.x;
-    if (bid < T.n_band_blocks) {
-        band_block<M, true>(P, T, bid, smem);
-        return;
-    }
-    bid -= T.n_band_blocks;
+    const int bid = blockIdx.x;
     if (bid < T.n_tile_blocks) {
         const TileKind k = classify(P, T, bid);
         if (k.generic) edge_tile<M, true>(P, T, k.x0, k.z0, k.x_end, smem);
@@ -796,12 +665,7 @@ template <int M>
 __global__ void __launch_bounds__(kThreads, 5) stress_kernel(const __grid_constant__ StepParams P, const __grid_constant__ TiledArgs T,
                                                           const __grid_constant__ StrMaps maps) {
     extern __shared__ __align__(128) float smem[];
-    int bid = blockIdx.x;
-    if (bid < T.n_band_blocks) {
-        band_block<M, false>(P, T, bid, smem);
-        return;
-    }
-    bid -= T.n_band_blocks;
+    const int bid = blockIdx.x;
     if (bid < T.n_tile_blocks) {
         const TileKind k = classify(P, T, bid);
         if (k.generic) edge_tile<M, false>(P, T, k.x0, k.z0, k.x_end, smem);
@@ -811,6 +675,125 @@ __global__ void __launch_bounds__(kThreads, 5) stress_kernel(const __grid_consta
 
 // Receivers of the last step (the velocity launch of step k records k-1).
 __global__ void record_kernel(const StepParams P) { record_block(P, blockIdx.x); }
+
+// ---------------------------------------------------------------- bottom band
+// Rows nz-nbc-1 .. nz-2: the bottom edge and the two bottom corners, whose
+// HABC rules form a recurrence along j (each row reads the final values of
+// the row above, nz-nbc-2 first, which the tiles stored).  The tiles left the
+// stencil values of these rows (before the HABC) in the band scratch, so all
+// that runs here is the recurrence.  One warp per (strip of kStripW columns,
+// output field) marches down the rows: lane l holds column xs-2+l, so lanes
+// 2..29 are the strip, lanes 1 and 30 carry the recurrence of the
+// neighbouring columns, and lanes 0 and 31 supply values only.  Stencil and
+// step-start values arrive by cp.async, kMarchRows rows per chunk, one chunk
+// ahead.  A lane's column fixes its rule for every row: rim columns keep the
+// stencil value; the bottom edge reads the final value of row j-1 (z term);
+// corner cells add the x term of their neighbour towards the interior
+// (stencil value, phase A); the last bottom-left column (nbc) and
+// bottom-right chunk starts redo it with that neighbour's final value
+// (phase B).  Both rules are evaluated and selected, so a warp never
+// diverges.  Lane 1's values are wrong only when its column is a
+// bottom-right chunk start and lane 30's only when its column is nbc; no
+// strip lane reads either then.
+
+// 4-byte asynchronous global -> shared copy; valid == false writes zero.
+__device__ __forceinline__ void cp_async4(float* dst, const float* src, bool valid) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(smem_u32(dst)), "l"(src), "r"(valid ? 4 : 0)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+constexpr int kMaxBandTab = 1024;                  // nbc + 2 <= this
+constexpr int kMarchStage = 2 * 2 * kMarchRows * 32;  // two chunks of (stencil, step-start) values
+
+// Band-pass warps of one half step: strips x 3 (a velocity pass leaves the
+// third field's warps idle).
+__host__ __device__ constexpr int band_warp_count(int nx) { return band_block_count(nx) * 3; }
+
+template <bool VEL>
+__device__ void band_march(const StepParams& P, const TiledArgs& T, int item, float* stage, float* stab) {
+    constexpr unsigned FULL = 0xffffffffu;
+    const int strip = item / 3, f = item % 3;
+    if (VEL && f == 2) return;  // block-uniform
+    const int lane = threadIdx.x & 31;
+    const int b = P.nbc, nx = P.nx, nz = P.nz, r0 = nx - b - 1, j0 = nz - b - 1;
+    const float* tab = P.w_tab[VEL ? f : 2];
+    for (int d = lane; d < b + 2; d += 32) stab[d] = __ldg(tab + d);
+    __syncwarp();
+    const int i = strip * kStripW - 2 + lane;
+    const bool col_ok = i >= 0 && i < nx;
+    const int q = VEL ? VX + f : TXX + f;
+    const float* oin = in_field(P, q);
+    float* oout = q == VX ? P.out[VX] : q == VZ ? P.out[VZ] : q == TXX ? P.out[TXX] : q == TZZ ? P.out[TZZ] : P.out[TXZ];
+    // the lane's rule
+    const bool rim = i <= 0 || i >= nx - 1;
+    const bool left = i >= 1 && i <= b;
+    const bool corner = left || (i >= r0 && i <= nx - 2);
+    const bool redo = i == b || (i > r0 - 1 && i <= nx - 2 && right_chunk_start(nx, b, i));
+    const int nb = min(max(lane + (left ? 1 : -1), 0), 31);  // neighbour towards the interior
+    const int dxi = max(min(i, nx - 1 - i), 0);
+    const size_t pitch = P.pitch;
+
+    auto stage_chunk = [&](int c) {
+        float* buf = stage + (c & 1) * (2 * kMarchRows * 32);
+        for (int r = 0; r < kMarchRows; ++r) {
+            const int jb = c * kMarchRows + r;
+            const bool ok = col_ok && jb < b;
+            cp_async4(buf + r * 32 + lane, ok ? band_pre_at(P, T, f, jb, i) : T.band_pre, ok);
+            cp_async4(buf + (kMarchRows + r) * 32 + lane, ok ? oin + cell(P, i, j0 + jb) : oin, ok);
+        }
+        cp_async_commit();
+    };
+    float fprev = col_ok ? oout[cell(P, i, j0 - 1)] : 0.f;  // final and step-start values of the row above
+    float ovp = col_ok ? __ldg(oin + cell(P, i, j0 - 1)) : 0.f;
+    float* dst = oout + (col_ok ? cell(P, i, j0) : 0);
+    const bool store = col_ok && lane >= 2 && lane < 2 + kStripW;
+    const int n_chunks = (b + kMarchRows - 1) / kMarchRows;
+    stage_chunk(0);
+    for (int c = 0; c < n_chunks; ++c) {
+        if (c + 1 < n_chunks) {
+            stage_chunk(c + 1);
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
+        }
+        __syncwarp();
+        const float* buf = stage + (c & 1) * (2 * kMarchRows * 32);
+        const int rows = min(kMarchRows, b - c * kMarchRows);
+#pragma unroll 4
+        for (int r = 0; r < rows; ++r) {
+            const int j = j0 + c * kMarchRows + r;
+            const float pv = buf[r * 32 + lane];
+            const float ov = buf[(kMarchRows + r) * 32 + lane];
+            const float w = stab[min(min(dxi, nz - 1 - j), b + 1)];
+            const float pv_nb = __shfl_sync(FULL, pv, nb);
+            const float ov_nb = __shfl_sync(FULL, ov, nb);
+            const float sz = edge_sum(P.qz, P.qt_z, P.qxt, fprev, ov, ovp);
+            const float fc = blend_corner(w, pv, edge_sum(P.qx, P.qt_x, P.qxt, pv_nb, ov, ov_nb), sz);
+            const float fe = blend_edge(w, pv, sz);
+            const float fa = rim ? pv : (corner ? fc : fe);
+            const float fa_nb = __shfl_sync(FULL, fa, nb);
+            const float fb = blend_corner(w, pv, edge_sum(P.qx, P.qt_x, P.qxt, fa_nb, ov, ov_nb), sz);
+            const float fin = redo ? fb : fa;
+            if (store) *dst = fin;
+            dst += pitch;
+            fprev = fin;
+            ovp = ov;
+        }
+        __syncwarp();  // every lane is done with this chunk's buffer
+    }
+}
+
+// The band pass of one half step: one warp per (strip, field) (P, T as for
+// the half step's tile launch, which must have completed).
+template <bool VEL>
+__global__ void __launch_bounds__(32) band_kernel(const __grid_constant__ StepParams P, const __grid_constant__ TiledArgs T) {
+    __shared__ __align__(16) float stage[kMarchStage];
+    __shared__ float stab[kMaxBandTab];
+    band_march<VEL>(P, T, blockIdx.x, stage, stab);
+}
 
 // Buoyancy dtx/rho_vx, dtz/rho_vx, dtx/rho_vz, dtz/rho_vz: the divisions of
 // update_velocity! (velocity.jl:41-42), IEEE-rounded, once per medium and dt.
@@ -828,15 +811,13 @@ __global__ void buoyancy_kernel(const float* rho_vx, const float* rho_vz, float 
 // Shared-memory bytes of one launch (the largest block role).
 template <int M>
 __host__ size_t tiled_smem_bytes(bool vel, int nbc, bool iso) {
+    (void)nbc;  // the bottom band runs in its own launch
     using G = Geo<M>;
     const int nin = vel ? 3 : 2, nout = vel ? 2 : 3;
     const int npoint = vel ? (iso ? 4 : 6) : 6;
     const size_t interior = ((size_t)nin * G::BOXS + (size_t)npoint * kPBox) * 4 + 16;
     const size_t edge = ((size_t)nin * (G::RW + 2 * M) * (G::RH + 2 * M) + (size_t)nout * G::RW * G::RH) * 4;
-    const int C = kBandW + 6, R = nbc + 1;
-    const size_t band = (std::max((size_t)nin * (C + 2 * M) * (R + 2 * M), (size_t)nout * R * C) +
-                         (size_t)nout * R * C + 2 * (size_t)nout * (kBandW + 2)) * 4;
-    return std::max(interior, std::max(edge, band));
+    return std::max(interior, edge);
 }
 
 }  // namespace fomo

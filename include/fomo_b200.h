@@ -187,7 +187,8 @@ int fomo_b200_shot_finish(uint64_t shot_handle, float* gather_out, FomoRunStats*
 
 /* Per-kernel timing of a shot's loop (no reference counterpart; used by
  * bench.py for the roofline).  Runs up to n_steps more steps of the shot
- * with CUDA events around every launch and reports, per kernel kind, the
+ * with CUDA events around every launch and reports, per kernel kind
+ * (velocity, stress, band_velocity, band_stress: max_kinds >= 4), the
  * launches, their summed device time and the algorithmic DRAM bytes of one
  * launch (the bytes a launch must move at minimum: each array it reads
  * once and each array it writes once, over the cells it updates). */
@@ -215,8 +216,9 @@ int fomo_b200_shot_profile(uint64_t shot_handle, int32_t n_steps, FomoKernelTime
  * every GPU loading the library holds until the process exits; grids whose
  * scratch does not fit are rejected with FOMO_EINVAL and a message giving
  * the bytes needed.  The scratch is 10 fields (+2 buoyancy arrays when
- * dtx == dtz, +4 otherwise) of pitch*nz floats plus a few KB, so for example a
- * 1000 x 1000 padded grid with dtx == dtz fits.
+ * dtx == dtz, +4 otherwise) of pitch*nz floats, 3*nbc rows of pitch floats
+ * for the bottom band, plus a few KB, so for example a 1000 x 1000 padded
+ * grid with dtx == dtz and nbc = 50 fits.
  *
  * Inputs: the five medium arrays on the device (each pitch*nz floats, row
  * pitch `pitch` floats: a multiple of 4 and >= round_up(nx, 4); 16-byte

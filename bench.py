@@ -47,6 +47,10 @@ def parse():
     p.add_argument("--cpu-seconds", type=float, default=15.0)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-batched", action="store_true", help="skip the batched-shots section")
+    p.add_argument("--no-serving", action="store_true", help="skip the serving section")
+    p.add_argument("--batch-nt", type=int, default=None, help="override nt of the batched section (development)")
+    p.add_argument("--serve-requests", type=int, default=24)
     return p.parse_args()
 
 
@@ -121,6 +125,7 @@ def host_inputs(w):
     nx, nz = w.nx_in + 2 * pad, w.nz_in + 2 * pad
     v_ref = F.julia_mean(w.vp) if w.vp.size <= 4_000_000 else np.float32(w.vp.mean(dtype=np.float64))
     habc = F.init_habc(nx, nz, w.nbc, w.dt, w.dx, w.dz, v_ref)
+    habc_v_ref = v_ref
     params = F.sim_params(w.dt, w.nt, w.dx, w.dz, w.fd_order)
     a = F.get_fd_coefficients(w.fd_order)
     wav = F.ricker_wavelet(w.f0, w.dt, w.nt)
@@ -128,7 +133,8 @@ def host_inputs(w):
     sj = F.coord_to_index(w.src_z[0], w.dz, pad)
     ri = np.rint(w.rec_x.astype(np.float32) / np.float32(w.dx)).astype(np.int32) + pad + 1
     rj = np.rint(w.rec_z.astype(np.float32) / np.float32(w.dz)).astype(np.int32) + pad + 1
-    return dict(pad=pad, nx=nx, nz=nz, arrays=(rho_vx, rho_vz, lam, mu, mu_txz), habc=habc, params=params,
+    return dict(pad=pad, nx=nx, nz=nz, arrays=(rho_vx, rho_vz, lam, mu, mu_txz), habc=habc, habc_v_ref=habc_v_ref,
+                params=params,
                 a=a, wav=wav, si=si, sj=sj, ri=ri, rj=rj)
 
 
@@ -186,6 +192,154 @@ def reference_arm(args, rank, world):
         "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------- batched and served shots
+def batched_section(args):
+    """64 shots on one 2000 x 800 medium: sequential plain shots
+    (fomo_b200_run_shot, one after another) against one fomo_b200_run_batch
+    call.  Shots/hour from the host clock around each call (inputs resident,
+    gathers copied to the host)."""
+    import fomo_julia_b200 as F
+    from fomo_julia_b200 import synthetic
+    B = F.backend("b200")
+    w = synthetic.batched_layered()
+    nt = args.batch_nt or w.nt
+    med = F.init_medium(w.vp, w.vs, w.rho, w.dx, w.dz, w.nbc, w.fd_order, B, free_surface=w.free_surface)
+    H = F.init_habc(med.nx, med.nz, w.nbc, w.dt, w.dx, w.dz, F.julia_mean(w.vp), B)
+    params = F.sim_params(w.dt, nt, w.dx, w.dz, w.fd_order)
+    a = F.get_fd_coefficients(w.fd_order)
+    wav = F.ricker_wavelet(w.f0, w.dt, nt)
+    rec = F.setup_receivers(w.rec_x, w.rec_z, med, type="vz")
+    cfg = F.multi_shot_config(w.src_x, w.src_z, wav)
+    W = F.Wavefield(med.nx, med.nz, B)
+    n_plain = 4
+    src0 = F.create_source(med, cfg.shots[0], wav)
+    F.run_shot(B, W, med, H, a, src0, rec, F.sim_params(w.dt, 64, w.dx, w.dz, w.fd_order))  # warm-up
+    plain, plain_dev = [], []
+    for k in range(n_plain):
+        src = F.create_source(med, cfg.shots[k], wav)
+        t0 = time.perf_counter()
+        r = F.run_shot(B, W, med, H, a, src, rec, params)
+        plain.append((time.perf_counter() - t0, r.gather))
+        plain_dev.append(r.stats["device_ms"] / 1e3)
+    W.release()
+    warm = F.multi_shot_config(w.src_x[:8], w.src_z[:8], wav[:64])
+    F.run_batch(B, med, H, a, rec, warm, F.sim_params(w.dt, 64, w.dx, w.dz, w.fd_order))  # warm-up
+    t0 = time.perf_counter()
+    res = F.run_batch(B, med, H, a, rec, cfg, params)
+    t_batch = time.perf_counter() - t0
+    med.release()
+    same = all(np.array_equal(res[k].gather, plain[k][1]) for k in range(n_plain))
+    t_plain = float(np.mean([t for t, _ in plain]))
+    cells = med.nx * med.nz
+    n = len(cfg.shots)
+    return {
+        "workload": f"{w.name}" + ("" if nt == w.nt else f" (nt {nt})"), "shots": n, "nt": nt,
+        "grid_padded": [med.nx, med.nz],
+        "plain_s_per_shot": t_plain, "plain_device_s_per_shot": float(np.mean(plain_dev)),
+        "plain_shots_per_hour": 3600.0 / t_plain, "plain_sample": f"first {n_plain} shots, one after another",
+        "batched_s": t_batch, "batched_device_s": res[0].stats["device_ms"] / 1e3,
+        "batched_shots_per_hour": n * 3600.0 / t_batch,
+        "speedup_vs_plain": (n * 3600.0 / t_batch) / (3600.0 / t_plain),
+        "batched_gcell_steps_s": n * cells * nt / t_batch / 1e9,
+        "batched_launches": res[0].stats["kernel_launches"],
+        "gathers_identical_to_plain": bool(same),
+    }
+
+
+def serving_section(args, c1):
+    """A Poisson stream of shot requests over six resident media (600x300,
+    1200x500, 2400x1000, 3200x1400, 2000x800 and the 4444x3819 medium),
+    order 8, nt ~ U[1500, 6000], 100..1000 receivers, served by one
+    ShotServer with a 150 GB budget.  Sequential plain time per request is
+    its medium's measured single-shot step time times nt."""
+    import threading
+    import fomo_julia_b200 as F
+    from fomo_julia_b200 import synthetic
+    B = F.backend("b200")
+    dt = 0.0008
+    media = []
+    for (vp, vs, rho), dx in synthetic.uneven_media():
+        media.append((vp, vs, rho, dx))
+    w2 = synthetic.batched_layered()
+    media.append((w2.vp, w2.vs, w2.rho, w2.dx))
+    M, Hs, recs_x = [], [], []
+    for vp, vs, rho, dx in media:
+        m = F.init_medium(vp, vs, rho, dx, dx, 50, 8, B, free_surface=True)
+        M.append(m)
+        Hs.append(F.init_habc(m.nx, m.nz, 50, dt, dx, dx, F.julia_mean(vp), B))
+    M.append(c1["medium"])
+    Hs.append(F.init_habc(c1["medium"].nx, c1["medium"].nz, 50, dt, 10.0, 10.0, c1["v_ref"], B))
+    dxs = [m.dx for m in M]
+    nx_in = [m.nx - 2 * m.pad for m in M]
+    a = F.get_fd_coefficients(8)
+    # plain step time per medium: one single shot of 200 steps
+    plain_step = []
+    for m, H in zip(M, Hs):
+        W = F.Wavefield(m.nx, m.nz, B)
+        wav = F.ricker_wavelet(12.0, dt, 200)
+        src = F.Source(m.nx // 2, m.pad + 2, wav)
+        rec = F.setup_receivers(np.linspace(0, (m.nx - 2 * m.pad - 1) * m.dx, 500).astype(np.float32),
+                                np.full(500, 10.0, np.float32), m)
+        F.run_shot(B, W, m, H, a, src, rec, F.sim_params(dt, 200, m.dx, m.dz, 8))
+        r = F.run_shot(B, W, m, H, a, src, rec, F.sim_params(dt, 200, m.dx, m.dz, 8))
+        plain_step.append(r.stats["device_ms"] / 1e3 / 200)
+        W.release()
+    n = args.serve_requests
+    probe = synthetic.serving_requests(n, nx_in, dxs, 1.0)
+    plain_total = sum(plain_step[q.medium] * q.nt for q in probe)
+    rate = 4.0 * n / plain_total  # offered load: four times what sequential plain shots sustain
+    reqs = synthetic.serving_requests(n, nx_in, dxs, rate)
+    budget = 150 << 30
+    try:
+        import torch
+        free, _ = torch.cuda.mem_get_info()
+        budget = min(budget, int(0.85 * free))
+    except Exception:
+        pass
+    results = [None] * n
+    with F.ShotServer(hbm_budget_bytes=budget) as srv:
+        tickets = [None] * n
+        t_start = time.perf_counter()
+
+        def submitter():
+            for k, q in enumerate(reqs):
+                d = q.arrival_s - (time.perf_counter() - t_start)
+                if d > 0:
+                    time.sleep(d)
+                m = M[q.medium]
+                wav = F.ricker_wavelet(q.f0, dt, q.nt)
+                src = F.Source(F.coord_to_index(q.src_x, m.dx, m.pad), F.coord_to_index(q.src_z, m.dz, m.pad), wav)
+                xs = np.linspace(0, (nx_in[q.medium] - 1) * m.dx, q.n_rec).astype(np.float32)
+                rec = F.setup_receivers(xs, np.full(q.n_rec, 10.0, np.float32), m)
+                tickets[k] = srv.submit(m, Hs[q.medium], a, src, rec, F.sim_params(dt, q.nt, m.dx, m.dz, 8), k)
+
+        th = threading.Thread(target=submitter)
+        th.start()
+        th.join()
+        for k in range(n):
+            results[k] = srv.wait(tickets[k])
+        makespan = time.perf_counter() - t_start
+        st = srv.stats()
+    for m in M[:-1]:
+        m.release()
+    lat = [r.stats["latency_ms"] for r in results]
+    cell_steps = sum((M[q.medium].nx * M[q.medium].nz) * q.nt for q in reqs)
+    from fomo_julia_b200.serving import percentile
+    return {
+        "requests": n, "media": [[m.nx, m.nz] for m in M], "arrival_rate_per_s": rate,
+        "arrival": "Poisson, rate = 4 x the sequential plain capacity of this request mix",
+        "hbm_budget_bytes": budget, "makespan_s": makespan,
+        "p50_latency_ms": percentile(lat, 50), "p99_latency_ms": percentile(lat, 99),
+        "served_shots_per_hour": n * 3600.0 / makespan,
+        "plain_shots_per_hour": n * 3600.0 / plain_total,
+        "speedup_vs_plain": plain_total / makespan,
+        "served_gcell_steps_s": cell_steps / makespan / 1e9,
+        "plain_us_per_step_by_medium": [round(t * 1e6, 2) for t in plain_step],
+        "peak_shots": st["peak_shots"], "peak_bytes": st["peak_bytes"], "kernel_launches": st["kernel_launches"],
+        "graph_replays": st["graph_replays"],
+    }
 
 
 # ---------------------------------------------------------------- B200 arm
@@ -347,7 +501,19 @@ def b200_arm(args, rank, world, local):
                "sample": f"first {n} time steps of the same shot ({t:.1f} s), C++ restatement of the "
                          f"reference's Float32 CPU path (oracle/), OpenMP"}
 
-    call("fomo_b200_wavefield_destroy", wf)
+    batched = served = None
+    if rank == 0 and world == 1:
+        call("fomo_b200_wavefield_destroy", wf)
+        wf = None
+        if not args.no_batched:
+            batched = batched_section(args)
+        if not args.no_serving:
+            pad = hi["pad"]
+            c1_medium = F.Medium(nx, nz, float(w.dx), float(w.dz), 0.0, 0.0, w.fd_order // 2, pad,
+                                 bool(w.free_surface), None, None, None, None, None, handle=med)
+            served = serving_section(args, {"medium": c1_medium, "v_ref": hi["habc_v_ref"]})
+    if wf is not None:
+        call("fomo_b200_wavefield_destroy", wf)
     call("fomo_b200_medium_destroy", med)
     if rank == 0:
         line = {
@@ -361,6 +527,7 @@ def b200_arm(args, rank, world, local):
             "loop_ms_per_shot": [round(t.device_ms, 2) for t in st_v],
             "e2e": e2e, "gpu_launches": int(launches), "clocks": clocks, "roofline": roofline,
             "cpu_baseline": cpu,
+            "batched": batched, "serving": served,
         }
         print(json.dumps(line), flush=True)
     if world > 1:

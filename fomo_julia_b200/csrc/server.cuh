@@ -8,9 +8,10 @@
 //   admit   queued requests, in arrival order, while their device bytes fit
 //           the HBM budget (and the shot limit); allocate and upload each
 //           shot, starting it at the next batch step;
-//   run     K batch steps: per FD order, a velocity tile launch and its band
-//           pass, a stress tile launch and its band pass, each over every
-//           shot in flight (step_batch.cuh), then the step-counter advance;
+//   run     K batch steps: per FD order (and up to 16 media), the step
+//           records, a velocity tile launch and its band pass, a stress tile
+//           launch and its band pass, each over every shot in flight
+//           (step_batch.cuh), then the step-counter advance;
 //           K steps are one CUDA graph replay once captured;
 //   retire  shots whose nt steps are done: record the last step's receivers,
 //           copy the gather to pinned memory, free the shot's memory (stream
@@ -68,7 +69,7 @@ class PinnedPool {
 
 enum ReqState { kQueued = 0, kRunning = 1, kDone = 2, kFailed = 3, kCancelled = 4 };
 
-// Buoyancy and descriptors of a medium for one (dtx, dtz), shared by the
+// Buoyancy and tile descriptors of a medium for one (dtx, dtz), shared by the
 // server's shots on it.
 struct Resident {
     Medium* med = nullptr;
@@ -76,8 +77,8 @@ struct Resident {
     int iso = 0;
     float* buoy = nullptr;
     const float* b[4] = {nullptr, nullptr, nullptr, nullptr};
-    CUtensorMap bmap[4];
-    CUtensorMap mod[3];
+    CUtensorMap bmap[4];  // tile boxes of the buoyancy arrays
+    CUtensorMap mod[3];   // tile boxes of lam, mu_txx, mu_txz
     int refs = 0;
     size_t bytes = 0;
 };
@@ -106,6 +107,8 @@ struct Request {
     int start = 0;           // batch step of the shot's step 1
     size_t band_off = 0, tabs_off = 0, cells_off = 0, wav_off = 0, gather_off = 0;
     fomo::ShotDev dev;       // host image of the shot's table entry
+    CUtensorMap halo[2][5];  // halo boxes (Geo<M>) of every field of both copies
+    CUtensorMap tile[2][5];  // tile boxes of every field of both copies
     void* staging = nullptr; // pinned: gather + status word
     cudaEvent_t done_ev = nullptr;
 };
@@ -170,30 +173,33 @@ int set_batch_smem(int M, size_t v, size_t s) {
     return fail(FOMO_EINVAL, "M=%d not supported", M);
 }
 
-template <int M>
-void launch_batch_M(bool vel, const fomo::BatchArgs& B, int grid, size_t smem, cudaStream_t st) {
-    if (vel) fomo::batch_velocity_kernel<M><<<grid, fomo::kThreads, smem, st>>>(B);
-    else fomo::batch_stress_kernel<M><<<grid, fomo::kThreads, smem, st>>>(B);
-}
-
-void launch_batch(int M, bool vel, const fomo::BatchArgs& B, int grid, size_t smem, cudaStream_t st) {
-    switch (M) {
-        case 1: launch_batch_M<1>(vel, B, grid, smem, st); break;
-        case 2: launch_batch_M<2>(vel, B, grid, smem, st); break;
-        case 3: launch_batch_M<3>(vel, B, grid, smem, st); break;
-        case 4: launch_batch_M<4>(vel, B, grid, smem, st); break;
-        case 5: launch_batch_M<5>(vel, B, grid, smem, st); break;
-        case 6: launch_batch_M<6>(vel, B, grid, smem, st); break;
-    }
-}
 
 // The shots of one FD order in flight: their launches of one step.
 struct LaunchSet {
     int M = 0;
     fomo::BatchArgs args{};
+    std::shared_ptr<fomo::BatchVelMaps> mv;  // descriptors of the set's shots (kernel parameters)
+    std::shared_ptr<fomo::BatchStrMaps> ms;
     int grid_v = 0, grid_s = 0, grid_b = 0;  // velocity tiles + receivers, stress tiles, band passes
     size_t smem_v = 0, smem_s = 0;
 };
+
+template <int M>
+void launch_batch_M(bool vel, const LaunchSet& S, cudaStream_t st) {
+    if (vel) fomo::batch_velocity_kernel<M><<<S.grid_v, fomo::kThreads, S.smem_v, st>>>(S.args, *S.mv);
+    else fomo::batch_stress_kernel<M><<<S.grid_s, fomo::kThreads, S.smem_s, st>>>(S.args, *S.ms);
+}
+
+void launch_batch(bool vel, const LaunchSet& S, cudaStream_t st) {
+    switch (S.M) {
+        case 1: launch_batch_M<1>(vel, S, st); break;
+        case 2: launch_batch_M<2>(vel, S, st); break;
+        case 3: launch_batch_M<3>(vel, S, st); break;
+        case 4: launch_batch_M<4>(vel, S, st); break;
+        case 5: launch_batch_M<5>(vel, S, st); break;
+        case 6: launch_batch_M<6>(vel, S, st); break;
+    }
+}
 
 class Server {
   public:
@@ -488,42 +494,18 @@ class Server {
     }
 
     template <int M>
-    int build_maps(Request& r, float* const (&field)[2][5]) {
+    static int build_maps(Request& r, float* const (&field)[2][5]) {
         using G = fomo::Geo<M>;
         const Medium& m = *r.med;
-        CUtensorMap halo[2][5], tile[2][5];
         for (int c = 0; c < 2; ++c)
             for (int q = 0; q < 5; ++q) {
-                if (int rc = encode_map(&halo[c][q], field[c][q], m.nx, m.nz, m.pitch, G::BOXW, G::BOXH)) return rc;
-                if (int rc = encode_map(&tile[c][q], field[c][q], m.nx, m.nz, m.pitch, fomo::kTX, fomo::kTZ)) return rc;
+                if (int rc = encode_map(&r.halo[c][q], field[c][q], m.nx, m.nz, m.pitch, G::BOXW, G::BOXH)) return rc;
+                if (int rc = encode_map(&r.tile[c][q], field[c][q], m.nx, m.nz, m.pitch, fomo::kTX, fomo::kTZ)) return rc;
             }
-        const Resident& R = *r.res;
-        for (int a = 0; a < 2; ++a) {
-            const int b = 1 - a;
-            fomo::VelMaps& vm = r.dev.vmap[a];
-            vm.xx = halo[a][fomo::TXX];
-            vm.zz = halo[a][fomo::TZZ];
-            vm.xz = halo[a][fomo::TXZ];
-            vm.vx = tile[a][fomo::VX];
-            vm.vz = tile[a][fomo::VZ];
-            vm.b0 = R.bmap[0];
-            vm.b1 = R.bmap[1];
-            vm.b2 = R.bmap[2];
-            vm.b3 = R.bmap[3];
-            fomo::StrMaps& sm = r.dev.smap[a];
-            sm.vx = halo[b][fomo::VX];
-            sm.vz = halo[b][fomo::VZ];
-            sm.txx = tile[a][fomo::TXX];
-            sm.tzz = tile[a][fomo::TZZ];
-            sm.txz = tile[a][fomo::TXZ];
-            sm.lam = R.mod[0];
-            sm.mu = R.mod[1];
-            sm.mxz = R.mod[2];
-        }
         return FOMO_OK;
     }
 
-    int build_maps_any(Request& r, float* const (&field)[2][5]) {
+    static int build_maps_any(Request& r, float* const (&field)[2][5]) {
         switch (r.M) {
             case 1: return build_maps<1>(r, field);
             case 2: return build_maps<2>(r, field);
@@ -655,37 +637,53 @@ class Server {
         });
         sets_.clear();
         struct Part {
-            size_t shots_off = 0, groups_off = 0, rec_off = 0;
-            std::vector<fomo::GroupDev> groups;
+            size_t shots_off = 0, steps_off = 0, rec_off = 0;
             std::vector<int> rec;
             size_t n0 = 0, n = 0;
         };
         std::vector<Part> parts;
         size_t bytes = 0;
+        // One launch set per run of at most kShotsPerLaunch shots with the
+        // same M.
         for (size_t i = 0; i < order.size();) {
-            size_t j = i;
-            while (j < order.size() && order[j]->M == order[i]->M) ++j;
             Part p;
             p.n0 = i;
-            p.n = j - i;
             LaunchSet S;
             S.M = order[i]->M;
-            int band = 0, tile = 0;
-            for (size_t g = i; g < j;) {
-                size_t h = g;
-                while (h < j && order[h]->med == order[g]->med) ++h;
-                const Launch L = shape_of(*order[g]);
-                fomo::GroupDev G;
-                G.first = (int)(g - i);
-                G.n = (int)(h - g);
+            int band = 0, tile = 0, n_groups = 0;
+            size_t j = i;
+            while (j < order.size() && order[j]->M == S.M && n_groups < fomo::kMaxGroups &&
+                   j - i < (size_t)fomo::kShotsPerLaunch) {
+                size_t h = j;
+                while (h < order.size() && order[h]->M == S.M && order[h]->med == order[j]->med &&
+                       h - i < (size_t)fomo::kShotsPerLaunch)
+                    ++h;
+                const Launch L = shape_of(*order[j]);
+                fomo::GroupDev& G = S.args.groups[n_groups++];
+                G.first = (int)(j - i);
+                G.n = (int)(h - j);
                 G.n_band = L.n_band;
                 G.n_tile = L.n_tile;
                 G.band_off = band;
                 G.tile_off = tile;
                 band += G.n * G.n_band;
                 tile += G.n * G.n_tile;
-                p.groups.push_back(G);
-                g = h;
+                j = h;
+            }
+            p.n = j - i;
+            S.mv = std::make_shared<fomo::BatchVelMaps>();
+            S.ms = std::make_shared<fomo::BatchStrMaps>();
+            for (size_t k = i; k < j; ++k) {
+                const Request& r = *order[k];
+                const size_t t = k - i;
+                for (int c = 0; c < 2; ++c) {
+                    for (int f = 0; f < 3; ++f) S.mv->tau[t][c][f] = r.halo[c][fomo::TXX + f];
+                    for (int f = 0; f < 2; ++f) S.mv->v[t][c][f] = r.tile[c][fomo::VX + f];
+                    for (int f = 0; f < 2; ++f) S.ms->v[t][c][f] = r.halo[c][fomo::VX + f];
+                    for (int f = 0; f < 3; ++f) S.ms->tau[t][c][f] = r.tile[c][fomo::TXX + f];
+                }
+                for (int q = 0; q < 4; ++q) S.mv->b[t][q] = r.res->bmap[q];
+                for (int q = 0; q < 3; ++q) S.ms->mod[t][q] = r.res->mod[q];
             }
             int rec = 0;
             p.rec.push_back(0);
@@ -698,7 +696,7 @@ class Server {
                 S.smem_s = std::max(S.smem_s, L.smem_s);
             }
             S.args.n_shots = (int)p.n;
-            S.args.n_groups = (int)p.groups.size();
+            S.args.n_groups = n_groups;
             S.args.total_band = band;
             S.args.total_tile = tile;
             S.grid_v = tile + rec;
@@ -706,8 +704,8 @@ class Server {
             S.grid_b = band;
             p.shots_off = bytes;
             bytes += align_up(p.n * sizeof(fomo::ShotDev), 256);
-            p.groups_off = bytes;
-            bytes += align_up(p.groups.size() * sizeof(fomo::GroupDev), 256);
+            p.steps_off = bytes;
+            bytes += align_up(p.n * sizeof(fomo::ShotStep), 256);
             p.rec_off = bytes;
             bytes += align_up(p.rec.size() * sizeof(int), 256);
             parts.push_back(std::move(p));
@@ -729,11 +727,10 @@ class Server {
             fomo::ShotDev* sd = reinterpret_cast<fomo::ShotDev*>(h + p.shots_off);
             for (size_t k = 0; k < p.n; ++k)
                 std::memcpy((void*)&sd[k], (const void*)&order[p.n0 + k]->dev, sizeof(fomo::ShotDev));
-            std::memcpy(h + p.groups_off, p.groups.data(), p.groups.size() * sizeof(fomo::GroupDev));
             std::memcpy(h + p.rec_off, p.rec.data(), p.rec.size() * sizeof(int));
             LaunchSet& S = sets_[s];
             S.args.shots = reinterpret_cast<const fomo::ShotDev*>(d_tables_ + p.shots_off);
-            S.args.groups = reinterpret_cast<const fomo::GroupDev*>(d_tables_ + p.groups_off);
+            S.args.steps = reinterpret_cast<fomo::ShotStep*>(d_tables_ + p.steps_off);
             S.args.rec_off = reinterpret_cast<const int*>(d_tables_ + p.rec_off);
             S.args.step = d_step_;
             if (int rc = set_batch_smem(S.M, S.smem_v, S.smem_s)) return rc;
@@ -766,12 +763,14 @@ class Server {
     }
 
     // ------------------------------------------------------------ stepping
-    int launches_per_step() const { return 4 * (int)sets_.size() + 1; }
+    int launches_per_step() const { return 5 * (int)sets_.size() + 1; }
 
     void enqueue_step() {
-        for (const LaunchSet& S : sets_) launch_batch(S.M, true, S.args, S.grid_v, S.smem_v, st_);
+        for (const LaunchSet& S : sets_)
+            fomo::batch_prep_kernel<<<(S.args.n_shots + 127) / 128, 128, 0, st_>>>(S.args);
+        for (const LaunchSet& S : sets_) launch_batch(true, S, st_);
         for (const LaunchSet& S : sets_) fomo::batch_band_kernel<true><<<S.grid_b, 32, 0, st_>>>(S.args);
-        for (const LaunchSet& S : sets_) launch_batch(S.M, false, S.args, S.grid_s, S.smem_s, st_);
+        for (const LaunchSet& S : sets_) launch_batch(false, S, st_);
         for (const LaunchSet& S : sets_) fomo::batch_band_kernel<false><<<S.grid_b, 32, 0, st_>>>(S.args);
         fomo::batch_advance_kernel<<<1, 1, 0, st_>>>(d_step_);
     }

@@ -20,17 +20,20 @@
 //
 // Every block runs the single-shot code (edge_tile, fast_vel, fast_str,
 // record_block, band_march) on its shot's parameters, so a batched shot's
-// results are bit-identical to the same shot run alone.
+// results are bit-identical to the same shot run alone.  The TMA descriptors
+// of a launch's shots travel in its kernel parameters (BatchVelMaps,
+// BatchStrMaps): descriptors kept in global memory would need a proxy fence
+// per descriptor in every block.
 #pragma once
+
+#include <cstddef>
 
 #include "step_tiled.cuh"
 
 namespace fomo {
 
 // One shot of a batch (device memory, written by the host).
-struct alignas(64) ShotDev {
-    VelMaps vmap[2];        // by input copy a: tau(a) halo boxes, v(a), buoyancy
-    StrMaps smap[2];        // by input copy a: v(1-a) halo boxes, tau(a), moduli
+struct ShotDev {
     StepParams P;           // static part; in/out, src_w and rec_k are set per launch
     TiledArgs T;            // block counts, buoyancy, status word
     float* field[2][5];     // the two copies of the five fields
@@ -48,13 +51,37 @@ struct GroupDev {
     int band_off, tile_off; // first band / tile block of the group in its launch
 };
 
+// Per-shot state of the current batch step, written by batch_prep_kernel.
+struct ShotStep {
+    int ks;        // local step (may lie outside 1..nt)
+    float src_w;   // wavelet sample of step ks (0 outside the wavelet)
+    int pad_[2];
+};
+
+constexpr int kMaxGroups = 16;       // media per launch
+constexpr int kShotsPerLaunch = 16;  // shots per launch (the host splits larger batches)
+
+// TMA descriptors of a launch's shots, passed as kernel parameters (by
+// shot s of the launch and wavefield copy c).
+struct BatchVelMaps {
+    CUtensorMap tau[kShotsPerLaunch][2][3];  // halo boxes of txx, tzz, txz
+    CUtensorMap v[kShotsPerLaunch][2][2];    // tile boxes of vx, vz
+    CUtensorMap b[kShotsPerLaunch][4];       // tile boxes of the four buoyancy arrays
+};
+struct BatchStrMaps {
+    CUtensorMap v[kShotsPerLaunch][2][2];    // halo boxes of vx, vz
+    CUtensorMap tau[kShotsPerLaunch][2][3];  // tile boxes of txx, tzz, txz
+    CUtensorMap mod[kShotsPerLaunch][3];     // tile boxes of lam, mu_txx, mu_txz
+};
+
 struct BatchArgs {
     const ShotDev* shots;
-    const GroupDev* groups;
+    ShotStep* steps;        // [n_shots]
     const int* rec_off;     // [n_shots + 1]: first receiver block of each shot
     const int* step;        // batch step of this launch (1-based)
     int n_shots, n_groups;
     int total_band, total_tile;
+    GroupDev groups[kMaxGroups];  // by value: decoded from the constant bank
 };
 
 struct BatchItem {
@@ -66,16 +93,17 @@ struct BatchItem {
 template <bool TILE>
 __device__ __forceinline__ BatchItem in_groups(const BatchArgs& B, int b) {
     int g = 0;
+#pragma unroll 1
     for (int h = 1; h < B.n_groups; ++h) {
         const int off = TILE ? B.groups[h].tile_off : B.groups[h].band_off;
         if (off <= b) g = h;
     }
-    const GroupDev G = B.groups[g];
-    const int r = b - (TILE ? G.tile_off : G.band_off);
+    const int r = b - (TILE ? B.groups[g].tile_off : B.groups[g].band_off);
+    const int n = B.groups[g].n;
     BatchItem it;
     it.role = TILE ? 1 : 0;
-    it.shot = G.first + r % G.n;
-    it.local = r / G.n;
+    it.shot = B.groups[g].first + r % n;
+    it.local = r / n;
     return it;
 }
 
@@ -102,67 +130,50 @@ __device__ __forceinline__ BatchItem decode(const BatchArgs& B, int bid, bool ve
 struct BatchBlock {
     StepParams P;
     TiledArgs T;
-    BatchItem it;
+    float* field[2][5];
+    ShotStep st;
     int a;       // input copy
-    int ks;      // local step (0 = block idle)
 };
 
-// Orders the host's copy of a shot table entry before the TMA unit reads the
-// descriptor from global memory (issued by the thread that issues the loads).
-__device__ __forceinline__ void tensormap_acquire(const CUtensorMap* m) {
-    asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(m) : "memory");
-}
-
-// Thread 0 decodes the block; all threads copy the shot's parameters; thread 0
-// then sets the per-step fields.  Returns false for an idle block.
+// Every thread decodes the block from the kernel parameters; thread 0 reads
+// the shot's step record while all threads copy its parameters (one round
+// trip to memory); thread 0 then sets the per-step fields.  Returns false for
+// an idle block.
 template <bool VEL, bool BAND>
-__device__ __forceinline__ bool setup_block(const BatchArgs& B, BatchBlock& bb) {
-    if (threadIdx.x == 0) {
-        bb.ks = 0;
-        bb.it = decode(B, blockIdx.x, VEL, BAND);
-        if (bb.it.role >= 0) {
-            const ShotDev& sd = B.shots[bb.it.shot];
-            const int ks = *B.step - sd.start + 1;
-            const bool run = bb.it.role == 2 ? (ks >= 2 && ks <= sd.nt + 1) : (ks >= 1 && ks <= sd.nt);
-            if (run) bb.ks = ks;
-        }
-    }
+__device__ __forceinline__ bool setup_block(const BatchArgs& B, BatchBlock& bb, BatchItem& it) {
+    it = decode(B, blockIdx.x, VEL, BAND);
+    if (it.role < 0) return false;  // block-uniform
+    const ShotDev& sd = B.shots[it.shot];
+    static_assert(offsetof(ShotDev, T) == offsetof(ShotDev, P) + sizeof(StepParams) &&
+                      offsetof(ShotDev, field) == offsetof(ShotDev, T) + sizeof(TiledArgs) &&
+                      offsetof(BatchBlock, T) == sizeof(StepParams) &&
+                      offsetof(BatchBlock, field) == sizeof(StepParams) + sizeof(TiledArgs),
+                  "contiguous parameter copy");
+    constexpr int W = (int)((sizeof(StepParams) + sizeof(TiledArgs) + sizeof(sd.field)) / 4);
+    const int* src = reinterpret_cast<const int*>(&sd.P);
+    int* dst = reinterpret_cast<int*>(&bb.P);
+    if (threadIdx.x == 0) bb.st = B.steps[it.shot];
+    for (int w = threadIdx.x; w < W; w += blockDim.x) dst[w] = src[w];
     __syncthreads();
-    if (bb.ks == 0) return false;
-    const ShotDev& sd = B.shots[bb.it.shot];
-    static_assert(sizeof(StepParams) % 4 == 0 && sizeof(TiledArgs) % 4 == 0, "word copies");
-    {
-        const int* src = reinterpret_cast<const int*>(&sd.P);
-        int* dst = reinterpret_cast<int*>(&bb.P);
-        for (int w = threadIdx.x; w < (int)(sizeof(StepParams) / 4); w += blockDim.x) dst[w] = src[w];
-        const int* srt = reinterpret_cast<const int*>(&sd.T);
-        int* dtt = reinterpret_cast<int*>(&bb.T);
-        for (int w = threadIdx.x; w < (int)(sizeof(TiledArgs) / 4); w += blockDim.x) dtt[w] = srt[w];
-    }
-    __syncthreads();
+    const int ks = bb.st.ks;
+    const bool run = it.role == 2 ? (ks >= 2 && ks <= bb.P.nt + 1) : (ks >= 1 && ks <= bb.P.nt);
+    if (!run) return false;  // block-uniform
     if (threadIdx.x == 0) {
-        const int ks = bb.ks;
         const int a = (ks - 1) & 1, b = 1 - a;
         bb.a = a;
-        bb.P.src_w = (ks <= sd.n_wavelet) ? sd.wavelet[ks - 1] : 0.f;
-        for (int q = 0; q < 5; ++q) bb.P.in[q] = sd.field[a][q];
+        bb.P.src_w = bb.st.src_w;
+        for (int q = 0; q < 5; ++q) bb.P.in[q] = bb.field[a][q];
         for (int q = 0; q < 5; ++q) bb.P.out[q] = nullptr;
-        if (bb.it.role == 1) {
-            const CUtensorMap* m = VEL ? reinterpret_cast<const CUtensorMap*>(&sd.vmap[a])
-                                       : reinterpret_cast<const CUtensorMap*>(&sd.smap[a]);
-            const int n = VEL ? (int)(sizeof(VelMaps) / sizeof(CUtensorMap)) : (int)(sizeof(StrMaps) / sizeof(CUtensorMap));
-            for (int t = 0; t < n; ++t) tensormap_acquire(m + t);
-        }
         if (VEL) {
             // reads v(a), tau(a); writes v(b); records step ks-1 from copy a
-            bb.P.out[VX] = sd.field[b][VX];
-            bb.P.out[VZ] = sd.field[b][VZ];
+            bb.P.out[VX] = bb.field[b][VX];
+            bb.P.out[VZ] = bb.field[b][VZ];
             bb.P.rec_k = ks - 1;
         } else {
             // reads v(b) (new), tau(a); writes tau(b)
-            bb.P.in[VX] = sd.field[b][VX];
-            bb.P.in[VZ] = sd.field[b][VZ];
-            for (int q = 2; q < 5; ++q) bb.P.out[q] = sd.field[b][q];
+            bb.P.in[VX] = bb.field[b][VX];
+            bb.P.in[VZ] = bb.field[b][VZ];
+            for (int q = 2; q < 5; ++q) bb.P.out[q] = bb.field[b][q];
             bb.P.rec_k = 0;
         }
     }
@@ -170,33 +181,58 @@ __device__ __forceinline__ bool setup_block(const BatchArgs& B, BatchBlock& bb) 
     return true;
 }
 
+// Step records of every shot for the batch step *B.step (one thread each);
+// launched before the step's first launch.
+__global__ void batch_prep_kernel(const __grid_constant__ BatchArgs B) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= B.n_shots) return;
+    const ShotDev& sd = B.shots[s];
+    ShotStep st;
+    st.ks = *B.step - sd.start + 1;
+    st.src_w = (st.ks >= 1 && st.ks <= sd.n_wavelet) ? sd.wavelet[st.ks - 1] : 0.f;
+    st.pad_[0] = st.pad_[1] = 0;
+    B.steps[s] = st;
+}
+
 template <int M>
-__global__ void __launch_bounds__(kThreads, 5) batch_velocity_kernel(const __grid_constant__ BatchArgs B) {
+__global__ void __launch_bounds__(kThreads, 5) batch_velocity_kernel(const __grid_constant__ BatchArgs B,
+                                                                  const __grid_constant__ BatchVelMaps MV) {
     extern __shared__ __align__(128) float smem[];
     __shared__ BatchBlock bb;
-    if (!setup_block<true, false>(B, bb)) return;
+    BatchItem it;
+    if (!setup_block<true, false>(B, bb, it)) return;
     const StepParams& P = bb.P;
     const TiledArgs& T = bb.T;
-    if (bb.it.role == 1) {
-        const TileKind k = classify(P, T, bb.it.local);
+    if (it.role == 1) {
+        const TileKind k = classify(P, T, it.local);
         if (k.generic) edge_tile<M, true>(P, T, k.x0, k.z0, k.x_end, smem);
-        else fast_vel<M>(P, T, B.shots[bb.it.shot].vmap[bb.a], k.x0, k.z0, k.x_end, k.band, k.rim, smem);
+        else {
+            const int s = it.shot, a = bb.a;
+            const VelMapRefs mp{&MV.tau[s][a][0], &MV.tau[s][a][1], &MV.tau[s][a][2], &MV.v[s][a][0], &MV.v[s][a][1],
+                                &MV.b[s][0],      &MV.b[s][1],      &MV.b[s][2],      &MV.b[s][3]};
+            fast_vel<M>(P, T, mp, k.x0, k.z0, k.x_end, k.band, k.rim, smem);
+        }
     } else {
-        record_block(P, bb.it.local);
+        record_block(P, it.local);
     }
 }
 
 template <int M>
-__global__ void __launch_bounds__(kThreads, 5) batch_stress_kernel(const __grid_constant__ BatchArgs B) {
+__global__ void __launch_bounds__(kThreads, 5) batch_stress_kernel(const __grid_constant__ BatchArgs B,
+                                                                const __grid_constant__ BatchStrMaps MS) {
     extern __shared__ __align__(128) float smem[];
     __shared__ BatchBlock bb;
-    if (!setup_block<false, false>(B, bb)) return;
+    BatchItem it;
+    if (!setup_block<false, false>(B, bb, it)) return;
     const StepParams& P = bb.P;
     const TiledArgs& T = bb.T;
-    {
-        const TileKind k = classify(P, T, bb.it.local);
-        if (k.generic) edge_tile<M, false>(P, T, k.x0, k.z0, k.x_end, smem);
-        else fast_str<M>(P, T, B.shots[bb.it.shot].smap[bb.a], k.x0, k.z0, k.x_end, k.band, k.rim, smem);
+    const TileKind k = classify(P, T, it.local);
+    if (k.generic) edge_tile<M, false>(P, T, k.x0, k.z0, k.x_end, smem);
+    else {
+        const int s = it.shot, a = bb.a, b = 1 - a;
+        const StrMapRefs mp{&MS.v[s][b][0],   &MS.v[s][b][1],   &MS.tau[s][a][0], &MS.tau[s][a][1],
+                            &MS.tau[s][a][2], &MS.mod[s][0],    &MS.mod[s][1],    &MS.mod[s][2]};
+        fast_str<M>(P, T, mp, k.x0, k.z0, k.x_end, k.band, k.rim, smem);
     }
 }
 
@@ -207,13 +243,17 @@ __global__ void __launch_bounds__(32) batch_band_kernel(const __grid_constant__ 
     __shared__ __align__(16) float stage[kMarchStage];
     __shared__ float stab[kMaxBandTab];
     __shared__ BatchBlock bb;
-    if (!setup_block<VEL, true>(B, bb)) return;
-    band_march<VEL>(bb.P, bb.T, bb.it.local, stage, stab);
+    BatchItem it;
+    if (!setup_block<VEL, true>(B, bb, it)) return;
+    band_march<VEL>(bb.P, bb.T, it.local, stage, stab);
 }
 
 // Advances the batch step counter; launched once per step after the stress
 // launches of every order.
 __global__ void batch_advance_kernel(int* step) { *step += 1; }
+
+static_assert(sizeof(BatchArgs) + sizeof(BatchVelMaps) <= 32764 && sizeof(BatchArgs) + sizeof(BatchStrMaps) <= 32764,
+              "kernel parameters above the 32764-byte limit");
 
 // Static shared memory of a batch block (beyond the dynamic part).
 constexpr size_t kBatchStaticSmem = sizeof(BatchBlock);

@@ -90,6 +90,21 @@ struct VelMaps {
 struct StrMaps {
     CUtensorMap vx, vz, txx, tzz, txz, lam, mu, mxz;
 };
+// The descriptors a tile uses, wherever they live (kernel parameters only:
+// the TMA unit may cache descriptors, and parameter space needs no proxy
+// fence).
+struct VelMapRefs {
+    const CUtensorMap *xx, *zz, *xz, *vx, *vz, *b0, *b1, *b2, *b3;
+};
+struct StrMapRefs {
+    const CUtensorMap *vx, *vz, *txx, *tzz, *txz, *lam, *mu, *mxz;
+};
+__device__ __forceinline__ VelMapRefs refs_of(const VelMaps& m) {
+    return {&m.xx, &m.zz, &m.xz, &m.vx, &m.vz, &m.b0, &m.b1, &m.b2, &m.b3};
+}
+__device__ __forceinline__ StrMapRefs refs_of(const StrMaps& m) {
+    return {&m.vx, &m.vz, &m.txx, &m.tzz, &m.txz, &m.lam, &m.mu, &m.mxz};
+}
 
 constexpr int kErrTmaTimeout = 1;
 
@@ -131,6 +146,15 @@ __device__ __forceinline__ void tma_load_2d(float* dst, const CUtensorMap* map, 
         ::"r"(smem_u32(dst)), "l"((uint64_t)map), "r"(x), "r"(z), "r"(smem_u32(bar))
         : "memory");
 }
+
+// 4-byte asynchronous global -> shared copy; valid == false writes zero.
+__device__ __forceinline__ void cp_async4(float* dst, const float* src, bool valid) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(smem_u32(dst)), "l"(src), "r"(valid ? 4 : 0)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
 __device__ __forceinline__ float4 ldg4(const float* p) { return __ldg(reinterpret_cast<const float4*>(p)); }
 __device__ __forceinline__ void stg4(float* p, float4 v) { *reinterpret_cast<float4*>(p) = v; }
@@ -359,7 +383,7 @@ struct TilePre {
 };
 
 template <int M>
-__device__ __forceinline__ void fast_vel(const StepParams& P, const TiledArgs& T, const VelMaps& mp, int x0, int z0,
+__device__ __forceinline__ void fast_vel(const StepParams& P, const TiledArgs& T, const VelMapRefs& mp, int x0, int z0,
                                          int x_end, bool band, bool rim, float* smem) {
     using G = Geo<M>;
     constexpr int BOX = G::BOXS;
@@ -380,16 +404,16 @@ __device__ __forceinline__ void fast_vel(const StepParams& P, const TiledArgs& T
     __syncthreads();
     if (threadIdx.x == 0) {
         mbar_expect_tx(bar, (3 * G::BOXW * G::BOXH + (T.iso ? 4 : 6) * kPBox) * 4);
-        tma_load_2d(s_xx, &mp.xx, x0 - G::HX, z0 - M, bar);
-        tma_load_2d(s_zz, &mp.zz, x0 - G::HX, z0 - M, bar);
-        tma_load_2d(s_xz, &mp.xz, x0 - G::HX, z0 - M, bar);
-        tma_load_2d(p_vx, &mp.vx, x0, z0, bar);
-        tma_load_2d(p_vz, &mp.vz, x0, z0, bar);
-        tma_load_2d(p_b0, &mp.b0, x0, z0, bar);
-        tma_load_2d(p_b2, &mp.b2, x0, z0, bar);
+        tma_load_2d(s_xx, mp.xx, x0 - G::HX, z0 - M, bar);
+        tma_load_2d(s_zz, mp.zz, x0 - G::HX, z0 - M, bar);
+        tma_load_2d(s_xz, mp.xz, x0 - G::HX, z0 - M, bar);
+        tma_load_2d(p_vx, mp.vx, x0, z0, bar);
+        tma_load_2d(p_vz, mp.vz, x0, z0, bar);
+        tma_load_2d(p_b0, mp.b0, x0, z0, bar);
+        tma_load_2d(p_b2, mp.b2, x0, z0, bar);
         if (!T.iso) {
-            tma_load_2d(p_b1, &mp.b1, x0, z0, bar);
-            tma_load_2d(p_b3, &mp.b3, x0, z0, bar);
+            tma_load_2d(p_b1, mp.b1, x0, z0, bar);
+            tma_load_2d(p_b3, mp.b3, x0, z0, bar);
         }
     }
     if (!wait_tma(bar, T)) return;
@@ -478,7 +502,7 @@ __device__ __forceinline__ void fast_vel(const StepParams& P, const TiledArgs& T
 }
 
 template <int M>
-__device__ __forceinline__ void fast_str(const StepParams& P, const TiledArgs& T, const StrMaps& mp, int x0, int z0,
+__device__ __forceinline__ void fast_str(const StepParams& P, const TiledArgs& T, const StrMapRefs& mp, int x0, int z0,
                                          int x_end, bool band, bool rim, float* smem) {
     using G = Geo<M>;
     constexpr int BOX = G::BOXS;
@@ -498,14 +522,14 @@ __device__ __forceinline__ void fast_str(const StepParams& P, const TiledArgs& T
     __syncthreads();
     if (threadIdx.x == 0) {
         mbar_expect_tx(bar, (2 * G::BOXW * G::BOXH + 6 * kPBox) * 4);
-        tma_load_2d(s_vx, &mp.vx, x0 - G::HX, z0 - M, bar);
-        tma_load_2d(s_vz, &mp.vz, x0 - G::HX, z0 - M, bar);
-        tma_load_2d(p_xx, &mp.txx, x0, z0, bar);
-        tma_load_2d(p_zz, &mp.tzz, x0, z0, bar);
-        tma_load_2d(p_xz, &mp.txz, x0, z0, bar);
-        tma_load_2d(p_lam, &mp.lam, x0, z0, bar);
-        tma_load_2d(p_mu, &mp.mu, x0, z0, bar);
-        tma_load_2d(p_mxz, &mp.mxz, x0, z0, bar);
+        tma_load_2d(s_vx, mp.vx, x0 - G::HX, z0 - M, bar);
+        tma_load_2d(s_vz, mp.vz, x0 - G::HX, z0 - M, bar);
+        tma_load_2d(p_xx, mp.txx, x0, z0, bar);
+        tma_load_2d(p_zz, mp.tzz, x0, z0, bar);
+        tma_load_2d(p_xz, mp.txz, x0, z0, bar);
+        tma_load_2d(p_lam, mp.lam, x0, z0, bar);
+        tma_load_2d(p_mu, mp.mu, x0, z0, bar);
+        tma_load_2d(p_mxz, mp.mxz, x0, z0, bar);
     }
     if (!wait_tma(bar, T)) return;
 
@@ -655,7 +679,7 @@ __global__ void __launch_bounds__(kThreads, 5) velocity_kernel(const __grid_cons
     if (bid < T.n_tile_blocks) {
         const TileKind k = classify(P, T, bid);
         if (k.generic) edge_tile<M, true>(P, T, k.x0, k.z0, k.x_end, smem);
-        else fast_vel<M>(P, T, maps, k.x0, k.z0, k.x_end, k.band, k.rim, smem);
+        else fast_vel<M>(P, T, refs_of(maps), k.x0, k.z0, k.x_end, k.band, k.rim, smem);
         return;
     }
     record_block(P, bid - T.n_tile_blocks);
@@ -669,7 +693,7 @@ __global__ void __launch_bounds__(kThreads, 5) stress_kernel(const __grid_consta
     if (bid < T.n_tile_blocks) {
         const TileKind k = classify(P, T, bid);
         if (k.generic) edge_tile<M, false>(P, T, k.x0, k.z0, k.x_end, smem);
-        else fast_str<M>(P, T, maps, k.x0, k.z0, k.x_end, k.band, k.rim, smem);
+        else fast_str<M>(P, T, refs_of(maps), k.x0, k.z0, k.x_end, k.band, k.rim, smem);
     }
 }
 
@@ -696,14 +720,6 @@ __global__ void record_kernel(const StepParams P) { record_block(P, blockIdx.x);
 // bottom-right chunk start and lane 30's only when its column is nbc; no
 // strip lane reads either then.
 
-// 4-byte asynchronous global -> shared copy; valid == false writes zero.
-__device__ __forceinline__ void cp_async4(float* dst, const float* src, bool valid) {
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(smem_u32(dst)), "l"(src), "r"(valid ? 4 : 0)
-                 : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
 constexpr int kMaxBandTab = 1024;                  // nbc + 2 <= this
 constexpr int kMarchStage = 2 * 2 * kMarchRows * 32;  // two chunks of (stencil, step-start) values

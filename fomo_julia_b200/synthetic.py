@@ -124,3 +124,56 @@ def batched_layered(seed: int = 2) -> Workload:
     rec_x = np.arange(400) * 5 * dx
     return Workload("layered_2000x800_o8_nt4000_64shots", vp, vs, rho, dx, dx, 50, 8, True, 0.001, 4000, 12.0,
                     src_x, [12.5] * 64, rec_x.astype(f32), np.full(400, 12.5, dtype=f32), ["vz"])
+
+
+@dataclass
+class Request:
+    """One shot request of an uneven batch or a serving stream."""
+    medium: int          # index into the media list
+    src_x: float         # metres
+    src_z: float
+    nt: int
+    n_rec: int
+    f0: float
+    fd_order: int
+    arrival_s: float = 0.0
+
+
+UNEVEN_GRIDS = [(600, 300, 3), (1200, 500, 4), (2400, 1000, 5), (3200, 1400, 6)]  # (nx, nz, seed), dx = 10 m
+
+
+def uneven_media():
+    """The four layered media of the uneven batch: 600x300, 1200x500,
+    2400x1000 and 3200x1400 cells, dx = dz = 10 m, seeds 3..6."""
+    return [(layered(nx, nz, 10.0, seed), 10.0) for nx, nz, seed in UNEVEN_GRIDS]
+
+
+def uneven_requests(n: int = 48, seed: int = 7) -> List[Request]:
+    """48 shots over the uneven media: FD order 4, 8 or 12, nt ~ U[1500, 6000]
+    (dt 0.8 ms), 100..800 receivers, f0 ~ U[8, 15] Hz, source x uniform at
+    the surface (z = 10 m)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    out = []
+    for _ in range(n):
+        m = int(rng.integers(0, len(UNEVEN_GRIDS)))
+        nx = UNEVEN_GRIDS[m][0]
+        out.append(Request(m, float(rng.uniform(0, (nx - 1) * 10.0)), 10.0, int(rng.integers(1500, 6001)),
+                           int(rng.integers(100, 801)), float(rng.uniform(8.0, 15.0)),
+                           int(rng.choice([4, 8, 12]))))
+    return out
+
+
+def serving_requests(n: int, media_nx: List[int], media_dx: List[float], rate_per_s: float,
+                     seed: int = 8) -> List[Request]:
+    """A Poisson stream of shot requests over resident media: medium uniform,
+    source x uniform at z = 10 m, nt ~ U[1500, 6000], 100..1000 receivers,
+    order 8, 12 Hz; arrivals with exponential gaps of mean 1/rate_per_s."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    t = 0.0
+    out = []
+    for _ in range(n):
+        m = int(rng.integers(0, len(media_nx)))
+        out.append(Request(m, float(rng.uniform(0, (media_nx[m] - 1) * media_dx[m])), 10.0,
+                           int(rng.integers(1500, 6001)), int(rng.integers(100, 1001)), 12.0, 8, t))
+        t += float(rng.exponential(1.0 / rate_per_s))
+    return out

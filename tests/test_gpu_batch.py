@@ -210,3 +210,16 @@ def test_cancel_and_medium_in_use(b200):
     assert st["cancelled"] == 1 and st["completed"] == 3 and st["peak_shots"] == 1
     S.med.release()
     assert S.med.handle == 0
+
+
+def test_more_media_than_one_launch_holds(b200):
+    """18 media of one order: the server splits them over two launch sets."""
+    Ss = [setup(layered(30 + k, 24 + (k % 5), seed=40 + k, nbc=5, fd_order=8, nt=60), b200) for k in range(18)]
+    refs = [single(S, source(S, 100.0, 20.0), b200) for S in Ss]
+    with F.ShotServer() as srv:
+        ts = [srv.submit(S.med, S.H, S.a, source(S, 100.0, 20.0), S.rec, params_of(S)) for S in Ss]
+        out = [srv.wait(t, timeout=WAIT_S) for t in ts]
+    for r, g in zip(out, refs):
+        assert np.array_equal(r.gather, g)
+    for S in Ss:
+        S.med.release()

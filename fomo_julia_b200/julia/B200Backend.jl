@@ -187,4 +187,32 @@ function run_shots!(b::B200, W::Wavefield{B200Field}, M::Medium, H::HABCConfig, 
     results
 end
 
+"""Batched form of run_shots!: every shot of `shot_config` in one
+fomo_b200_run_batch call (shots side by side on the device); the gathers
+equal run_shots!'s bit for bit."""
+function run_shots_batched!(::B200, M::Medium, H::HABCConfig, a, rec_template::Receivers,
+                            shot_config::MultiShotConfig, params::SimParams)
+    med = M.rho_vx.medium
+    tv, tz, tt = weight_table(Array(H.w_vx), H.nbc), weight_table(Array(H.w_vz), H.nbc),
+                 weight_table(Array(H.w_tau), H.nbc)
+    coeffs = Vector{Float32}(a)
+    wav = Vector{Float32}(shot_config.wavelet)
+    ri, rj = Int32.(collect(rec_template.i)), Int32.(collect(rec_template.j))
+    srcs = [(_coord_to_index(s.source_x, M.dx, M.pad), _coord_to_index(s.source_z, M.dz, M.pad))
+            for s in shot_config.shots]
+    gathers = [zeros(Float32, params.nt, length(ri)) for _ in srcs]
+    GC.@preserve tv tz tt coeffs wav ri rj gathers begin
+        h = Ref(FomoHabc(H.nbc, H.qx, H.qz, H.qt_x, H.qt_z, H.qxt, pointer(tv), pointer(tz), pointer(tt)))
+        shots = [FomoShot(pointer(coeffs), params.M, params.dt, params.dtx, params.dtz, params.nt,
+                          si, sj, pointer(wav), length(wav), length(ri), pointer(ri), pointer(rj),
+                          rec_kind(rec_template.type)) for (si, sj) in srcs]
+        ptrs = [pointer(g) for g in gathers]
+        check(ccall((:fomo_b200_run_batch, LIB), Cint,
+                    (UInt64, Ref{FomoHabc}, Ptr{FomoShot}, Int32, Ptr{Ptr{Float32}}, Ptr{Cvoid}),
+                    med, h, shots, length(shots), ptrs, C_NULL))
+    end
+    [ShotResult(gathers[k], shot_config.shots[k].shot_id, Int(srcs[k][1]), Int(srcs[k][2]),
+                Vector{Int}(ri), Vector{Int}(rj)) for k in eachindex(srcs)]
+end
+
 end # module

@@ -8,10 +8,12 @@ from .elastic2d import (  # noqa: F401
     AbstractBackend, B200Backend, B200_BACKEND, backend, to_device, synchronize,
     DeviceArray, Medium, HABCConfig, Wavefield, Source, Receivers, SimParams, sim_params,
     TimeStepInfo, ShotResult, ShotConfig, MultiShotConfig, multi_shot_config,
-    get_fd_coefficients, ricker_wavelet, julia_mean, init_medium, init_habc, setup_receivers,
+    get_fd_coefficients, ricker_wavelet, julia_mean, init_medium, init_medium_device, init_habc, setup_receivers,
     coord_to_index, create_source, reset, run_shot, run_shots, run_batch, save_gather, load_gather,
     pad_array, compute_staggered_params, taylor_coefficients,
 )
 from .serving import ShotServer, Ticket, percentile  # noqa: F401
+from .geometry import (SurveyGeometry, MultiShotGeometry, create_geometry, save_geometry,  # noqa: F401
+                       julia_str)
 
 __version__ = "0.1.0"

@@ -98,6 +98,9 @@ SIGNATURES = {
     "fomo_b200_medium_create": [_I32, _I32, _I32, _I32, _I32, ctypes.c_float, ctypes.c_float,
                                 _P, _P, _P, _P, _P, ctypes.POINTER(_U64)],
     "fomo_b200_medium_destroy": [_U64],
+    "fomo_b200_medium_create_from_model": [_I32, _I32, _P, _P, _P, ctypes.c_float, ctypes.c_float, _I32, _I32, _I32,
+                                           ctypes.POINTER(_U64)],
+    "fomo_b200_medium_download": [_U64, _I32, _P],
     "fomo_b200_wavefield_create": [_I32, _I32, ctypes.POINTER(_U64)],
     "fomo_b200_wavefield_destroy": [_U64],
     "fomo_b200_wavefield_reset": [_U64],

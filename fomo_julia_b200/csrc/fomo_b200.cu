@@ -609,6 +609,66 @@ int fomo_b200_medium_create(int32_t nx, int32_t nz, int32_t M, int32_t pad, int3
     return FOMO_OK;
 }
 
+int fomo_b200_medium_create_from_model(int32_t nx_in, int32_t nz_in, const float* vp, const float* vs,
+                                       const float* rho, float dx, float dz, int32_t nbc, int32_t M,
+                                       int32_t free_surface, uint64_t* medium) {
+    std::lock_guard<std::mutex> lk(ctx().mu);
+    if (int rc = ensure_init()) return rc;
+    if (!medium || !vp || !vs || !rho) return fail(FOMO_EINVAL, "NULL pointer argument");
+    if (nx_in < 2 || nz_in < 2 || nbc < 1) return fail(FOMO_EINVAL, "bad model size %dx%d or nbc %d", nx_in, nz_in, nbc);
+    const int pad = nbc + M;
+    const int nx = nx_in + 2 * pad, nz = nz_in + 2 * pad;
+    if (int rc = check_medium_args(nx, nz, M, pad)) return rc;
+    if (free_surface && pad < 5) return fail(FOMO_EINVAL, "free surface needs pad >= 5 (rows pad-4..pad+1), got %d", pad);
+    auto m = std::make_unique<Medium>();
+    m->nx = nx;
+    m->nz = nz;
+    m->pitch = pitch_of(nx);
+    m->M = M;
+    m->pad = pad;
+    m->fs = free_surface ? 1 : 0;
+    m->dx = dx;
+    m->dz = dz;
+    const size_t plane = (size_t)m->pitch * nz;
+    const size_t model = (size_t)nx_in * nz_in;
+    float* d_model = nullptr;
+    cudaError_t e = cudaMalloc(&m->base, 5 * plane * sizeof(float));
+    if (e == cudaSuccess) e = cudaMalloc(&d_model, 3 * model * sizeof(float));
+    if (e != cudaSuccess) {
+        if (d_model) cudaFree(d_model);
+        return fail(FOMO_ENOMEM, "medium allocation failed: %s", cudaGetErrorString(e));
+    }
+    cudaStream_t st = ctx().stream;
+    const float* src[3] = {vp, vs, rho};
+    int rc = FOMO_OK;
+    for (int q = 0; q < 3 && rc == FOMO_OK; ++q)
+        if (cudaMemcpyAsync(d_model + q * model, src[q], model * sizeof(float), cudaMemcpyHostToDevice, st) != cudaSuccess)
+            rc = fail(FOMO_ECUDA, "model upload failed");
+    if (rc == FOMO_OK) {
+        fomo::ModelView V{d_model, d_model + model, d_model + 2 * model, nx_in, nz_in, pad};
+        fomo::medium_init_kernel<<<8 * 148, 256, 0, st>>>(V, nx, nz, m->pitch, m->base, m->base + plane,
+                                                          m->base + 2 * plane, m->base + 3 * plane, m->base + 4 * plane);
+        if (cudaGetLastError() != cudaSuccess) rc = fail(FOMO_ECUDA, "medium set-up kernel launch failed");
+    }
+    cudaStreamSynchronize(st);
+    cudaFree(d_model);
+    if (rc) return rc;
+    *medium = put(std::move(m));
+    return FOMO_OK;
+}
+
+int fomo_b200_medium_download(uint64_t medium, int32_t q, float* host) {
+    std::lock_guard<std::mutex> lk(ctx().mu);
+    if (int rc = ensure_init()) return rc;
+    Medium* m = get<Medium>(medium);
+    if (!m) return fail(FOMO_EINVAL, "unknown medium handle %llu", (unsigned long long)medium);
+    if (q < 0 || q > 4 || !host) return fail(FOMO_EINVAL, "bad array %d or NULL host pointer", q);
+    CUDA_TRY(cudaMemcpy2DAsync(host, m->nx * sizeof(float), m->arr(q), m->pitch * sizeof(float),
+                               m->nx * sizeof(float), m->nz, cudaMemcpyDeviceToHost, ctx().stream));
+    CUDA_TRY(cudaStreamSynchronize(ctx().stream));
+    return FOMO_OK;
+}
+
 int fomo_b200_medium_destroy(uint64_t medium) {
     std::lock_guard<std::mutex> lk(ctx().mu);
     if (int rc = ensure_init()) return rc;

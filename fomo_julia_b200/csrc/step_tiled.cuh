@@ -811,6 +811,49 @@ __global__ void __launch_bounds__(32) band_kernel(const __grid_constant__ StepPa
     band_march<VEL>(P, T, blockIdx.x, stage, stab);
 }
 
+// ---------------------------------------------------------------- medium set-up
+// init_medium on the device (init.jl:68-158): the (nx_in, nz_in) vp, vs, rho
+// padded by edge replication (_pad_array, init.jl:119-134: a padded cell takes
+// the model cell at its coordinates clamped into the model) and the staggered
+// parameters of _compute_staggered_params (init.jl:136-158), in its Float32
+// operation order:
+//   mu = rho * (vs * vs), lam = rho * (vp * vp) - 2 * mu, rho_vx = rho,
+//   rho_vz = 0.25 * (((rho[i,j] + rho[i+1,j]) + rho[i,j+1]) + rho[i+1,j+1]),
+//   mu_txz = 2 / (1 / mu[i,j] + 1 / mu[i,j+1]),
+// the last row and column of rho_vz and the last row of mu_txz copied from
+// their neighbours.  Outputs have row pitch `pitch`.
+struct ModelView {
+    const float *vp, *vs, *rho;  // (nx_in, nz_in), x fastest
+    int nx_in, nz_in, pad;
+    __device__ __forceinline__ size_t at(int i, int j) const {
+        const int ii = min(max(i - pad, 0), nx_in - 1), jj = min(max(j - pad, 0), nz_in - 1);
+        return (size_t)ii + (size_t)jj * nx_in;
+    }
+    __device__ __forceinline__ float mu(int i, int j) const {
+        const size_t k = at(i, j);
+        return fmul(__ldg(rho + k), fmul(__ldg(vs + k), __ldg(vs + k)));
+    }
+};
+
+__global__ void medium_init_kernel(const ModelView V, int nx, int nz, int pitch, float* rho_vx, float* rho_vz,
+                                   float* lam, float* mu_txx, float* mu_txz) {
+    const size_t n = (size_t)nx * nz;
+    for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
+        const int i = (int)(k % nx), j = (int)(k / nx);
+        const size_t m = V.at(i, j), o = (size_t)i + (size_t)j * pitch;
+        const float rho = __ldg(V.rho + m), vp = __ldg(V.vp + m);
+        const float mu = V.mu(i, j);
+        mu_txx[o] = mu;
+        lam[o] = fsub(fmul(rho, fmul(vp, vp)), fmul(2.f, mu));
+        rho_vx[o] = rho;
+        const int ic = min(i, nx - 2), jc = min(j, nz - 2);
+        const float r00 = __ldg(V.rho + V.at(ic, jc)), r10 = __ldg(V.rho + V.at(ic + 1, jc));
+        const float r01 = __ldg(V.rho + V.at(ic, jc + 1)), r11 = __ldg(V.rho + V.at(ic + 1, jc + 1));
+        rho_vz[o] = fmul(0.25f, fadd(fadd(fadd(r00, r10), r01), r11));
+        mu_txz[o] = fdiv(2.f, fadd(fdiv(1.f, V.mu(i, jc)), fdiv(1.f, V.mu(i, jc + 1))));
+    }
+}
+
 // Buoyancy dtx/rho_vx, dtz/rho_vx, dtx/rho_vz, dtz/rho_vz: the divisions of
 // update_velocity! (velocity.jl:41-42), IEEE-rounded, once per medium and dt.
 __global__ void buoyancy_kernel(const float* rho_vx, const float* rho_vz, float dtx, float dtz, size_t n,

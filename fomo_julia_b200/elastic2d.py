@@ -199,6 +199,12 @@ class Medium:
             self.handle = h.value
         return self.handle
 
+    def array(self, q: int) -> np.ndarray:
+        """Array q (0 rho_vx, 1 rho_vz, 2 lam, 3 mu_txx, 4 mu_txz) as the device holds it."""
+        out = np.zeros((self.nx, self.nz), dtype=f32, order="F")
+        call("fomo_b200_medium_download", self.upload(), int(q), out.ctypes.data)
+        return out
+
     def release(self) -> None:
         if self.handle:
             call("fomo_b200_medium_destroy", self.handle)
@@ -250,6 +256,30 @@ def init_medium(vp, vs, rho, dx, dz, nbc: int, fd_order: int, b: B200Backend = B
                rho_vx, rho_vz, lam, mu, mu_txz, device=b.device)
     m.upload()
     return m
+
+
+def init_medium_device(vp, vs, rho, dx, dz, nbc: int, fd_order: int, b: B200Backend = B200_BACKEND,
+                       free_surface: bool = True) -> Medium:
+    """init_medium with the padding and staggered parameters computed on the
+    GPU (fomo_b200_medium_create_from_model): the same medium bit for bit,
+    without the host-side set-up.  The returned Medium holds no host copies
+    (download them with Medium.array)."""
+    if fd_order % 2 or not 2 <= fd_order <= 12:
+        raise ValueError(f"Unsupported FD order: {fd_order}")
+    M = fd_order // 2
+    pad = nbc + M
+    arrs = [np.asfortranarray(a, dtype=f32) for a in (vp, vs, rho)]
+    if arrs[0].ndim != 2 or arrs[1].shape != arrs[0].shape or arrs[2].shape != arrs[0].shape:
+        raise ValueError("vp, vs and rho must be matrices of the same size")
+    nx_in, nz_in = arrs[0].shape
+    _lib.ensure_init(b.device)
+    h = ctypes.c_uint64(0)
+    call("fomo_b200_medium_create_from_model", nx_in, nz_in, *[a.ctypes.data for a in arrs], float(f32(dx)),
+         float(f32(dz)), int(nbc), M, int(free_surface), ctypes.byref(h))
+    x_max = float(f32((nx_in - 1) * float(f32(dx))))
+    z_max = float(f32((nz_in - 1) * float(f32(dz))))
+    return Medium(nx_in + 2 * pad, nz_in + 2 * pad, float(f32(dx)), float(f32(dz)), x_max, z_max, M, pad,
+                  bool(free_surface), None, None, None, None, None, handle=h.value, device=b.device)
 
 
 @dataclass

@@ -104,6 +104,21 @@ int fomo_b200_medium_create(int32_t nx, int32_t nz, int32_t M, int32_t pad,
                             const float* mu_txz, uint64_t* medium);
 int fomo_b200_medium_destroy(uint64_t medium);
 
+/* init_medium (src/utils/init.jl:68-99) on the device: uploads the unpadded
+ * (nx_in, nz_in) vp, vs, rho (host, column major) and computes the padding
+ * (_pad_array, init.jl:119-134; pad = nbc + M) and the staggered parameters
+ * (_compute_staggered_params, init.jl:136-158) in the GPU, with the same
+ * Float32 operations in the same order: the medium is bit-identical to
+ * fomo_b200_medium_create of the host-computed arrays, and three unpadded
+ * arrays cross PCIe instead of five padded ones. */
+int fomo_b200_medium_create_from_model(int32_t nx_in, int32_t nz_in, const float* vp,
+                                       const float* vs, const float* rho, float dx, float dz,
+                                       int32_t nbc, int32_t M, int32_t free_surface,
+                                       uint64_t* medium);
+/* Array(M.rho_vx) etc.: copies staggered array q (0 rho_vx, 1 rho_vz, 2 lam,
+ * 3 mu_txx, 4 mu_txz) into host[nx*nz]. */
+int fomo_b200_medium_download(uint64_t medium, int32_t q, float* host);
+
 /* ---------------------------------------------------------------------- */
 /* HABC: HABCConfig{T} (src/core/Structures.jl:94-105) as built by         */
 /* init_habc (src/utils/init.jl:171-203).                                  */

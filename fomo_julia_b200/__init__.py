@@ -13,6 +13,7 @@ from .elastic2d import (  # noqa: F401
     pad_array, compute_staggered_params, taylor_coefficients,
 )
 from .serving import ShotServer, Ticket, percentile  # noqa: F401
+from .snapshots import SnapshotRecorder, VideoConfig  # noqa: F401
 from .geometry import (SurveyGeometry, MultiShotGeometry, create_geometry, save_geometry,  # noqa: F401
                        julia_str)
 

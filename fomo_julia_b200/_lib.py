@@ -106,6 +106,7 @@ SIGNATURES = {
     "fomo_b200_wavefield_reset": [_U64],
     "fomo_b200_wavefield_download": [_U64, _I32, _P],
     "fomo_b200_wavefield_upload": [_U64, _I32, _P],
+    "fomo_b200_wavefield_snapshot": [_U64, _I32, _I32, _P],
     "fomo_b200_run_shot": [_U64, _U64, ctypes.POINTER(FomoHabc), ctypes.POINTER(FomoShot), _P,
                            ctypes.POINTER(FomoRunStats)],
     "fomo_b200_shot_begin": [_U64, _U64, ctypes.POINTER(FomoHabc), ctypes.POINTER(FomoShot),

@@ -84,9 +84,12 @@ struct Wavefield : Object {
     int map_M = 0;          // M the halo maps were made for (0 = none)
     CUtensorMap maps[2][5]; // halo boxes (Geo<map_M>) of every field of both copies
     CUtensorMap pmaps[2][5];// tile boxes of every field of both copies
+    float* snap = nullptr;  // frame buffer of fomo_b200_wavefield_snapshot
+    size_t snap_bytes = 0;
     float* field(int copy, int q) const { return base + ((size_t)copy * 5 + q) * pitch * nz; }
     ~Wavefield() override {
         if (base) cudaFree(base);
+        if (snap) cudaFree(snap);
     }
 };
 
@@ -744,6 +747,33 @@ int fomo_b200_wavefield_upload(uint64_t wavefield, int32_t field, const float* h
     if (field < 0 || field > 4 || !host) return fail(FOMO_EINVAL, "bad field %d or NULL host pointer", field);
     CUDA_TRY(cudaMemcpy2DAsync(w->field(w->cur, field), w->pitch * sizeof(float), host, w->nx * sizeof(float),
                                w->nx * sizeof(float), w->nz, cudaMemcpyHostToDevice, ctx().stream));
+    CUDA_TRY(cudaStreamSynchronize(ctx().stream));
+    return FOMO_OK;
+}
+
+int fomo_b200_wavefield_snapshot(uint64_t wavefield, int32_t kind, int32_t downsample, float* host) {
+    std::lock_guard<std::mutex> lk(ctx().mu);
+    if (int rc = ensure_init()) return rc;
+    Wavefield* w = get<Wavefield>(wavefield);
+    if (!w) return fail(FOMO_EINVAL, "unknown wavefield handle %llu", (unsigned long long)wavefield);
+    if (kind < 0 || kind > 3 || downsample < 1 || !host) return fail(FOMO_EINVAL, "bad snapshot arguments");
+    const int nx_d = (w->nx + downsample - 1) / downsample, nz_d = (w->nz + downsample - 1) / downsample;
+    const size_t bytes = (size_t)nx_d * nz_d * sizeof(float);
+    if (bytes > w->snap_bytes) {
+        if (w->snap) cudaFree(w->snap);
+        w->snap = nullptr;
+        w->snap_bytes = 0;
+        cudaError_t e = cudaMalloc(&w->snap, bytes);
+        if (e != cudaSuccess) return fail(FOMO_ENOMEM, "snapshot buffer of %zu bytes failed", bytes);
+        w->snap_bytes = bytes;
+    }
+    const int c = w->cur;
+    const float* f0 = kind == 0 ? w->field(c, fomo::TXX) : kind == 3 ? w->field(c, fomo::VZ) : w->field(c, fomo::VX);
+    const float* f1 = kind == 0 ? w->field(c, fomo::TZZ) : w->field(c, fomo::VZ);
+    fomo::snapshot_kernel<<<4 * 148, 256, 0, ctx().stream>>>(f0, f1, kind, w->nx, w->nz, w->pitch, downsample, nx_d,
+                                                             nz_d, w->snap);
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaMemcpyAsync(host, w->snap, bytes, cudaMemcpyDeviceToHost, ctx().stream));
     CUDA_TRY(cudaStreamSynchronize(ctx().stream));
     return FOMO_OK;
 }

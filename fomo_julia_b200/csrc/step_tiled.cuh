@@ -811,6 +811,28 @@ __global__ void __launch_bounds__(32) band_kernel(const __grid_constant__ StepPa
     band_march<VEL>(P, T, blockIdx.x, stage, stab);
 }
 
+// ---------------------------------------------------------------- snapshots
+// One frame of a wavefield for the on_step hook (video_recorder.jl:260-297):
+// frame (i, j) (1-based, nx_d = cld(nx, ds), nz_d = cld(nz, ds)) takes cell
+// (min((i-1)*ds+1, nx), min((j-1)*ds+1, nz)) of
+//   kind 0  p   = (txx + tzz) * 0.5
+//   kind 1  vel = sqrt(vx^2 + vz^2)
+//   kind 2  vx,   kind 3  vz.
+__global__ void snapshot_kernel(const float* f0, const float* f1, int kind, int nx, int nz, int pitch, int ds,
+                                int nx_d, int nz_d, float* out) {
+    const size_t n = (size_t)nx_d * nz_d;
+    for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
+        const int i = (int)(k % nx_d), j = (int)(k / nx_d);
+        const int is = min(i * ds, nx - 1), js = min(j * ds, nz - 1);
+        const size_t c = (size_t)is + (size_t)js * pitch;
+        float v;
+        if (kind == 0) v = fmul(fadd(f0[c], f1[c]), 0.5f);
+        else if (kind == 1) v = __fsqrt_rn(fadd(fmul(f0[c], f0[c]), fmul(f1[c], f1[c])));
+        else v = f0[c];
+        out[k] = v;
+    }
+}
+
 // ---------------------------------------------------------------- medium set-up
 // init_medium on the device (init.jl:68-158): the (nx_in, nz_in) vp, vs, rho
 // padded by edge replication (_pad_array, init.jl:119-134: a padded cell takes

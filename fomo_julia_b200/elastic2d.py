@@ -387,6 +387,20 @@ class Wavefield:
     tzz = property(lambda self: self.field("tzz"))
     txz = property(lambda self: self.field("txz"))
 
+    def snapshot(self, field: str = "p", downsample: int = 1) -> np.ndarray:
+        """One frame of the current state (fomo_b200_wavefield_snapshot):
+        field p, vel, vx or vz, every downsample-th cell; (cld(nx, ds),
+        cld(nz, ds)) Float32, column major."""
+        kinds = {"p": 0, "vel": 1, "vx": 2, "vz": 3}
+        if field not in kinds:
+            raise ValueError(f"Unknown field: {field}. Use p, vel, vx, or vz")
+        ds = int(downsample)
+        if ds < 1:
+            raise ValueError("downsample must be >= 1")
+        out = np.zeros((-(-self.nx // ds), -(-self.nz // ds)), dtype=f32, order="F")
+        call("fomo_b200_wavefield_snapshot", self.handle, kinds[field], ds, out.ctypes.data)
+        return out
+
     def release(self) -> None:
         if self.handle:
             call("fomo_b200_wavefield_destroy", self.handle)

@@ -154,6 +154,19 @@ int fomo_b200_wavefield_download(uint64_t wavefield, int32_t field, float* host)
 /* to_device into W.vx etc.: overwrites the current value of one field. */
 int fomo_b200_wavefield_upload(uint64_t wavefield, int32_t field, const float* host);
 
+/* Snapshot frames for an on_step hook: the frame extraction of the
+ * reference's video recorder (src/visualization/video_recorder.jl:260-297)
+ * done on the device.  kind: FOMO_SNAP_P ((txx+tzz)*0.5), FOMO_SNAP_VEL
+ * (sqrt(vx^2+vz^2)), FOMO_SNAP_VX, FOMO_SNAP_VZ; frame (i, j) (1-based) is
+ * cell (min((i-1)*ds+1, nx), min((j-1)*ds+1, nz)) of the current state;
+ * host receives cld(nx,ds) * cld(nz,ds) floats, column major.  No rendering:
+ * the frames go to the caller's buffer. */
+#define FOMO_SNAP_P   0
+#define FOMO_SNAP_VEL 1
+#define FOMO_SNAP_VX  2
+#define FOMO_SNAP_VZ  3
+int fomo_b200_wavefield_snapshot(uint64_t wavefield, int32_t kind, int32_t downsample, float* host);
+
 /* ---------------------------------------------------------------------- */
 /* One shot: Source (Structures.jl:116-120), Receivers (:127-132),         */
 /* SimParams (:143-155) and the FD coefficients (init.jl:13-29).           */

@@ -41,3 +41,33 @@ def test_device_medium_equals_host_medium(b200, kw):
     assert np.array_equal(g1, g2)
     host.release()
     dev.release()
+
+
+def test_snapshots_match_host_extraction(b200):
+    """Device frames equal the reference's _extract_frame! of the downloaded fields."""
+    c = layered(61, 43, seed=5, nbc=6, fd_order=8, nt=60)
+    med = F.init_medium(c.vp, c.vs, c.rho, c.dx, c.dz, c.nbc, c.fd_order, b200, free_surface=c.free_surface)
+    H = F.init_habc(med.nx, med.nz, c.nbc, c.dt, c.dx, c.dz, c.v_ref, b200)
+    params = F.sim_params(c.dt, 60, c.dx, c.dz, c.fd_order)
+    src = F.Source(med.nx // 2, med.pad + 3, F.ricker_wavelet(c.f0, c.dt, 60))
+    rec = F.setup_receivers(c.rec_x, c.rec_z, med, type=c.rec_type)
+    W = F.Wavefield(med.nx, med.nz, b200)
+    recd = F.SnapshotRecorder(F.VideoConfig(fields=["p", "vel", "vx", "vz"], skip=20, downsample=3))
+    seen = []
+
+    def hook(Wh, info):
+        recd(Wh, info)
+        vx, vz, txx, tzz = (Wh.field(n) for n in ("vx", "vz", "txx", "tzz"))
+        raw = {"p": (txx + tzz) * np.float32(0.5), "vel": np.sqrt(vx * vx + vz * vz), "vx": vx, "vz": vz}
+        if info.k % 20 == 0:
+            for f, a in raw.items():
+                want = a[::3, ::3]
+                assert np.array_equal(recd.frames[f][-1][2], want), (f, info.k)
+            seen.append(info.k)
+        return True
+
+    F.run_shot(b200, W, med, H, F.get_fd_coefficients(c.fd_order), src, rec, params, on_step=hook, step_chunk=10)
+    assert seen == [20, 40, 60]
+    assert recd.stack("p").shape == (3, -(-med.nx // 3), -(-med.nz // 3))
+    W.release()
+    med.release()

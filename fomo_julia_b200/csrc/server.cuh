@@ -106,7 +106,7 @@ struct Request {
     Resident* res = nullptr;
     int start = 0;           // batch step of the shot's step 1
     size_t band_off = 0, tabs_off = 0, cells_off = 0, wav_off = 0, gather_off = 0;
-    fomo::ShotDev dev;       // host image of the shot's table entry
+    fomo::BatchShot vel, str;  // the shot's launch-parameter images (velocity, stress)
     CUtensorMap halo[2][5];  // halo boxes (Geo<M>) of every field of both copies
     CUtensorMap tile[2][5];  // tile boxes of every field of both copies
     void* staging = nullptr; // pinned: gather + status word
@@ -150,11 +150,11 @@ size_t batch_smem_any(int M, bool vel, int nbc, bool iso) {
 template <int M>
 int set_batch_smem_M(size_t v, size_t s) {
     std::lock_guard<std::mutex> lk(g_batch_attr_mu);
-    if (v > g_batch_smem[0][M] && v + fomo::kBatchStaticSmem > 48 * 1024) {
+    if (v > g_batch_smem[0][M] && v > 48 * 1024) {
         CUDA_TRY(cudaFuncSetAttribute(fomo::batch_velocity_kernel<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)v));
         g_batch_smem[0][M] = v;
     }
-    if (s > g_batch_smem[1][M] && s + fomo::kBatchStaticSmem > 48 * 1024) {
+    if (s > g_batch_smem[1][M] && s > 48 * 1024) {
         CUDA_TRY(cudaFuncSetAttribute(fomo::batch_stress_kernel<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s));
         g_batch_smem[1][M] = s;
     }
@@ -177,17 +177,16 @@ int set_batch_smem(int M, size_t v, size_t s) {
 // The shots of one FD order in flight: their launches of one step.
 struct LaunchSet {
     int M = 0;
-    fomo::BatchArgs args{};
-    std::shared_ptr<fomo::BatchVelMaps> mv;  // descriptors of the set's shots (kernel parameters)
-    std::shared_ptr<fomo::BatchStrMaps> ms;
-    int grid_v = 0, grid_s = 0, grid_b = 0;  // velocity tiles + receivers, stress tiles, band passes
+    std::shared_ptr<fomo::BatchVelLaunch> lv;  // kernel parameters of the velocity launches
+    std::shared_ptr<fomo::BatchStrLaunch> ls;  // and of the stress launches
+    int grid_v = 0, grid_s = 0, grid_b = 0;    // velocity tiles + receivers, stress tiles, band passes
     size_t smem_v = 0, smem_s = 0;
 };
 
 template <int M>
 void launch_batch_M(bool vel, const LaunchSet& S, cudaStream_t st) {
-    if (vel) fomo::batch_velocity_kernel<M><<<S.grid_v, fomo::kThreads, S.smem_v, st>>>(S.args, *S.mv);
-    else fomo::batch_stress_kernel<M><<<S.grid_s, fomo::kThreads, S.smem_s, st>>>(S.args, *S.ms);
+    if (vel) fomo::batch_velocity_kernel<M><<<S.grid_v, fomo::kThreads, S.smem_v, st>>>(*S.lv);
+    else fomo::batch_stress_kernel<M><<<S.grid_s, fomo::kThreads, S.smem_s, st>>>(*S.ls);
 }
 
 void launch_batch(bool vel, const LaunchSet& S, cudaStream_t st) {
@@ -260,8 +259,6 @@ class Server {
         ev_free_.clear();
         for (auto e : tev_free_) cudaEventDestroy(e);
         tev_free_.clear();
-        if (d_tables_ && st_) cudaFreeAsync(d_tables_, st_);
-        d_tables_ = nullptr;
         if (st_) cudaStreamSynchronize(st_);
         if (d_ctl_) cudaFree(d_ctl_);
         d_ctl_ = nullptr;
@@ -388,7 +385,6 @@ class Server {
     int64_t k_host_ = 0;          // batch steps enqueued
     bool dirty_ = true;           // membership changed since the tables were built
     std::vector<LaunchSet> sets_;
-    unsigned char* d_tables_ = nullptr;
     std::map<int, cudaGraphExec_t> graphs_;  // K -> graph of the current tables
     std::deque<cudaEvent_t> inflight_;
     std::vector<Deferred> deferred_;
@@ -575,7 +571,7 @@ class Server {
             for (int q = 0; q < 5; ++q) field[c][q] = reinterpret_cast<float*>(base + (size_t)(c * 5 + q) * plane);
         if (int e = build_maps_any(r, field)) return e;
 
-        fomo::StepParams& P = r.dev.P;
+        fomo::StepParams P;
         std::memset(&P, 0, sizeof(P));
         P.nx = m.nx;
         P.nz = m.nz;
@@ -607,7 +603,7 @@ class Server {
         P.rec_cell = reinterpret_cast<const int*>(base + r.cells_off);
         P.gather = r.d_gather;
         const Launch L = shape_of(r);
-        fomo::TiledArgs& T = r.dev.T;
+        fomo::TiledArgs T;
         std::memset(&T, 0, sizeof(T));
         for (int q = 0; q < 4; ++q) T.b[q] = r.res->b[q];
         T.iso = r.res->iso;
@@ -616,13 +612,29 @@ class Server {
         T.n_tile_blocks = L.n_tile;
         T.tiles_x = L.tiles_x;
         T.x_last = L.x_last;
-        for (int c = 0; c < 2; ++c)
-            for (int q = 0; q < 5; ++q) r.dev.field[c][q] = field[c][q];
-        r.dev.wavelet = reinterpret_cast<const float*>(base + r.wav_off);
-        r.dev.n_wavelet = (int)r.wavelet.size();
         r.start = (int)(k_host_ + 1);
-        r.dev.start = r.start;
-        r.dev.nt = r.nt;
+        for (fomo::BatchShot* S : {&r.vel, &r.str}) {
+            std::memset((void*)S, 0, sizeof(*S));
+            S->T = T;
+            S->wavelet = reinterpret_cast<const float*>(base + r.wav_off);
+            S->n_wavelet = (int)r.wavelet.size();
+            S->start = r.start;
+            S->nt = r.nt;
+        }
+        for (int c = 0; c < 2; ++c) {  // the step reads copy c, writes copy 1-c
+            const int o = 1 - c;
+            fomo::StepParams& V = r.vel.P[c];
+            V = P;
+            for (int q = 0; q < 5; ++q) V.in[q] = field[c][q];
+            V.out[fomo::VX] = field[o][fomo::VX];
+            V.out[fomo::VZ] = field[o][fomo::VZ];
+            fomo::StepParams& S = r.str.P[c];
+            S = P;
+            for (int q = 0; q < 5; ++q) S.in[q] = field[c][q];
+            S.in[fomo::VX] = field[o][fomo::VX];
+            S.in[fomo::VZ] = field[o][fomo::VZ];
+            for (int q = 2; q < 5; ++q) S.out[q] = field[o][q];
+        }
         return FOMO_OK;
     }
 
@@ -636,20 +648,17 @@ class Server {
             return x->med < y->med;
         });
         sets_.clear();
-        struct Part {
-            size_t shots_off = 0, steps_off = 0, rec_off = 0;
-            std::vector<int> rec;
-            size_t n0 = 0, n = 0;
-        };
-        std::vector<Part> parts;
-        size_t bytes = 0;
+        retire_graphs();
         // One launch set per run of at most kShotsPerLaunch shots with the
-        // same M.
+        // same M; everything it needs goes into its kernel parameters.
         for (size_t i = 0; i < order.size();) {
-            Part p;
-            p.n0 = i;
             LaunchSet S;
             S.M = order[i]->M;
+            S.lv = std::make_shared<fomo::BatchVelLaunch>();
+            S.ls = std::make_shared<fomo::BatchStrLaunch>();
+            std::memset((void*)S.lv.get(), 0, sizeof(fomo::BatchVelLaunch));
+            std::memset((void*)S.ls.get(), 0, sizeof(fomo::BatchStrLaunch));
+            fomo::BatchHead& H = S.lv->H;
             int band = 0, tile = 0, n_groups = 0;
             size_t j = i;
             while (j < order.size() && order[j]->M == S.M && n_groups < fomo::kMaxGroups &&
@@ -659,7 +668,7 @@ class Server {
                        h - i < (size_t)fomo::kShotsPerLaunch)
                     ++h;
                 const Launch L = shape_of(*order[j]);
-                fomo::GroupDev& G = S.args.groups[n_groups++];
+                fomo::GroupDev& G = H.groups[n_groups++];
                 G.first = (int)(j - i);
                 G.n = (int)(h - j);
                 G.n_band = L.n_band;
@@ -670,80 +679,39 @@ class Server {
                 tile += G.n * G.n_tile;
                 j = h;
             }
-            p.n = j - i;
-            S.mv = std::make_shared<fomo::BatchVelMaps>();
-            S.ms = std::make_shared<fomo::BatchStrMaps>();
+            int rec = 0;
+            H.rec_off[0] = 0;
             for (size_t k = i; k < j; ++k) {
                 const Request& r = *order[k];
                 const size_t t = k - i;
-                for (int c = 0; c < 2; ++c) {
-                    for (int f = 0; f < 3; ++f) S.mv->tau[t][c][f] = r.halo[c][fomo::TXX + f];
-                    for (int f = 0; f < 2; ++f) S.mv->v[t][c][f] = r.tile[c][fomo::VX + f];
-                    for (int f = 0; f < 2; ++f) S.ms->v[t][c][f] = r.halo[c][fomo::VX + f];
-                    for (int f = 0; f < 3; ++f) S.ms->tau[t][c][f] = r.tile[c][fomo::TXX + f];
-                }
-                for (int q = 0; q < 4; ++q) S.mv->b[t][q] = r.res->bmap[q];
-                for (int q = 0; q < 3; ++q) S.ms->mod[t][q] = r.res->mod[q];
-            }
-            int rec = 0;
-            p.rec.push_back(0);
-            for (size_t k = i; k < j; ++k) {
-                const Request& r = *order[k];
                 rec += (r.n_rec + fomo::kThreads - 1) / fomo::kThreads;
-                p.rec.push_back(rec);
+                H.rec_off[t + 1] = rec;
                 const Launch L = shape_of(r);
                 S.smem_v = std::max(S.smem_v, L.smem_v);
                 S.smem_s = std::max(S.smem_s, L.smem_s);
+                S.lv->shot[t] = r.vel;
+                S.ls->shot[t] = r.str;
+                for (int c = 0; c < 2; ++c) {
+                    for (int f = 0; f < 3; ++f) S.lv->tau[t][c][f] = r.halo[c][fomo::TXX + f];
+                    for (int f = 0; f < 2; ++f) S.lv->v[t][c][f] = r.tile[c][fomo::VX + f];
+                    for (int f = 0; f < 2; ++f) S.ls->v[t][c][f] = r.halo[c][fomo::VX + f];
+                    for (int f = 0; f < 3; ++f) S.ls->tau[t][c][f] = r.tile[c][fomo::TXX + f];
+                }
+                for (int q = 0; q < 4; ++q) S.lv->b[t][q] = r.res->bmap[q];
+                for (int q = 0; q < 3; ++q) S.ls->mod[t][q] = r.res->mod[q];
             }
-            S.args.n_shots = (int)p.n;
-            S.args.n_groups = n_groups;
-            S.args.total_band = band;
-            S.args.total_tile = tile;
+            H.step = d_step_;
+            H.n_shots = (int)(j - i);
+            H.n_groups = n_groups;
+            H.total_band = band;
+            H.total_tile = tile;
+            S.ls->H = H;
             S.grid_v = tile + rec;
             S.grid_s = tile;
             S.grid_b = band;
-            p.shots_off = bytes;
-            bytes += align_up(p.n * sizeof(fomo::ShotDev), 256);
-            p.steps_off = bytes;
-            bytes += align_up(p.n * sizeof(fomo::ShotStep), 256);
-            p.rec_off = bytes;
-            bytes += align_up(p.rec.size() * sizeof(int), 256);
-            parts.push_back(std::move(p));
+            if (int rc = set_batch_smem(S.M, S.smem_v, S.smem_s)) return rc;
             sets_.push_back(S);
             i = j;
-        }
-        // Replace the device tables (stream ordered: launches already queued
-        // keep reading the old ones until they are done).
-        if (d_tables_) CUDA_TRY(cudaFreeAsync(d_tables_, st_));
-        d_tables_ = nullptr;
-        retire_graphs();
-        if (sets_.empty()) return FOMO_OK;
-        if (cudaMallocFromPoolAsync(reinterpret_cast<void**>(&d_tables_), bytes, pool_, st_) != cudaSuccess)
-            return fail(FOMO_ENOMEM, "batch table allocation of %zu bytes failed", bytes);
-        unsigned char* h = static_cast<unsigned char*>(pinned_.take(bytes));
-        if (!h) return fail(FOMO_ENOMEM, "pinned staging of %zu bytes failed", bytes);
-        for (size_t s = 0; s < parts.size(); ++s) {
-            const Part& p = parts[s];
-            fomo::ShotDev* sd = reinterpret_cast<fomo::ShotDev*>(h + p.shots_off);
-            for (size_t k = 0; k < p.n; ++k)
-                std::memcpy((void*)&sd[k], (const void*)&order[p.n0 + k]->dev, sizeof(fomo::ShotDev));
-            std::memcpy(h + p.rec_off, p.rec.data(), p.rec.size() * sizeof(int));
-            LaunchSet& S = sets_[s];
-            S.args.shots = reinterpret_cast<const fomo::ShotDev*>(d_tables_ + p.shots_off);
-            S.args.steps = reinterpret_cast<fomo::ShotStep*>(d_tables_ + p.steps_off);
-            S.args.rec_off = reinterpret_cast<const int*>(d_tables_ + p.rec_off);
-            S.args.step = d_step_;
-            if (int rc = set_batch_smem(S.M, S.smem_v, S.smem_s)) return rc;
-        }
-        CUDA_TRY(cudaMemcpyAsync(d_tables_, h, bytes, cudaMemcpyHostToDevice, st_));
-        Deferred d;
-        d.ev = event();
-        d.pinned = h;
-        CUDA_TRY(cudaEventRecord(d.ev, st_));
-        deferred_.push_back(d);
-        {
-            std::lock_guard<std::mutex> lk(mu_);
-            stats_.h2d_bytes += (int64_t)bytes;
         }
         dirty_ = false;
         return FOMO_OK;
@@ -763,15 +731,15 @@ class Server {
     }
 
     // ------------------------------------------------------------ stepping
-    int launches_per_step() const { return 5 * (int)sets_.size() + 1; }
+    int launches_per_step() const { return 4 * (int)sets_.size() + 1; }
 
     void enqueue_step() {
-        for (const LaunchSet& S : sets_)
-            fomo::batch_prep_kernel<<<(S.args.n_shots + 127) / 128, 128, 0, st_>>>(S.args);
         for (const LaunchSet& S : sets_) launch_batch(true, S, st_);
-        for (const LaunchSet& S : sets_) fomo::batch_band_kernel<true><<<S.grid_b, 32, 0, st_>>>(S.args);
+        for (const LaunchSet& S : sets_)
+            fomo::batch_band_kernel<true, fomo::BatchVelLaunch><<<S.grid_b, 32, 0, st_>>>(*S.lv);
         for (const LaunchSet& S : sets_) launch_batch(false, S, st_);
-        for (const LaunchSet& S : sets_) fomo::batch_band_kernel<false><<<S.grid_b, 32, 0, st_>>>(S.args);
+        for (const LaunchSet& S : sets_)
+            fomo::batch_band_kernel<false, fomo::BatchStrLaunch><<<S.grid_b, 32, 0, st_>>>(*S.ls);
         fomo::batch_advance_kernel<<<1, 1, 0, st_>>>(d_step_);
     }
 
@@ -928,9 +896,7 @@ class Server {
     int retire(Request& r) {
         const size_t gbytes = (size_t)r.nt * r.n_rec * sizeof(float);
         if (r.n_rec > 0 && r.nt > 0) {  // receivers of the last step
-            fomo::StepParams P = r.dev.P;
-            const int c = r.nt & 1;  // copy written by step nt
-            for (int q = 0; q < 5; ++q) P.in[q] = r.dev.field[c][q];
+            fomo::StepParams P = r.vel.P[r.nt & 1];  // reads copy nt & 1: the state after step nt
             P.rec_k = r.nt;
             fomo::record_kernel<<<(r.n_rec + fomo::kThreads - 1) / fomo::kThreads, fomo::kThreads, 0, st_>>>(P);
             CUDA_TRY(cudaGetLastError());
@@ -1161,7 +1127,7 @@ int make_request(Medium* m, const FomoHabc* habc, const FomoShot* shot, float* g
     if (shot->n_rec > 0 && shot->nt > 0 && !gather_out) return fail(FOMO_EINVAL, "gather_out is NULL");
     const bool iso = shot->dtx == shot->dtz;
     const size_t smem = std::max(batch_smem_any(m->M, true, nbc, iso), batch_smem_any(m->M, false, nbc, iso));
-    if (smem + fomo::kBatchStaticSmem > 227 * 1024)
+    if (smem > 227 * 1024)
         return fail(FOMO_EINVAL, "nbc=%d needs %zu bytes of shared memory per block, more than 227 KB", nbc, smem);
     auto r = std::make_shared<Request>();
     r->med = m;

@@ -77,61 +77,15 @@ __device__ __forceinline__ const float* in_field(const StepParams& P, int q) {
 // source_receiver.jl:26-27) is applied to the values read, never stored, so
 // the stored fields keep the pre-injection values the HABC needs as f_old.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ float tau_in(const StepParams& P, int q, int i, int j) {
+// src_w is the wavelet sample of this step (P.src_w on the single-shot path).
+__device__ __forceinline__ float tau_in(const StepParams& P, int q, int i, int j, float src_w) {
     float v = __ldg(in_field(P, q) + cell(P, i, j));
-    if (q != TXZ && i == P.src_i && j == P.src_j) v = fadd(v, P.src_w);
+    if (q != TXZ && i == P.src_i && j == P.src_j) v = fadd(v, src_w);
     return v;
 }
 
 __device__ __forceinline__ bool in_stencil(const StepParams& P, int i, int j) {
     return i >= P.M && i <= P.nx - 1 - P.M && j >= P.M && j <= P.nz - 1 - P.M;
-}
-
-// Velocity after update_velocity! at (i, j), before the HABC.
-__device__ inline void vel_pre(const StepParams& P, int i, int j, float& vx, float& vz) {
-    const size_t c = cell(P, i, j);
-    vx = __ldg(P.in[VX] + c);
-    vz = __ldg(P.in[VZ] + c);
-    if (!in_stencil(P, i, j)) return;
-    float d1 = 0.f, d2 = 0.f, d3 = 0.f, d4 = 0.f;
-#pragma unroll 1
-    for (int l = 1; l <= P.M; ++l) {
-        const float al = P.a[l - 1];
-        d1 = fadd(fmul(al, fsub(tau_in(P, TXX, i + l - 1, j), tau_in(P, TXX, i - l, j))), d1);
-        d2 = fadd(fmul(al, fsub(tau_in(P, TXZ, i, j + l - 1), tau_in(P, TXZ, i, j - l))), d2);
-        d3 = fadd(fmul(al, fsub(tau_in(P, TXZ, i + l, j), tau_in(P, TXZ, i - l + 1, j))), d3);
-        d4 = fadd(fmul(al, fsub(tau_in(P, TZZ, i, j + l), tau_in(P, TZZ, i, j - l + 1))), d4);
-    }
-    const float rx = __ldg(P.rho_vx + c), rz = __ldg(P.rho_vz + c);
-    vx = fadd(vx, fadd(fmul(fdiv(P.dtx, rx), d1), fmul(fdiv(P.dtz, rx), d2)));
-    vz = fadd(vz, fadd(fmul(fdiv(P.dtx, rz), d3), fmul(fdiv(P.dtz, rz), d4)));
-}
-
-// Stress after update_stress! at (i, j), before the HABC.  P.in[VX], P.in[VZ]
-// are the velocities this step produced; P.in[TXX..TXZ] the stresses it read.
-__device__ inline void str_pre(const StepParams& P, int i, int j, float& txx, float& tzz, float& txz) {
-    txx = tau_in(P, TXX, i, j);
-    tzz = tau_in(P, TZZ, i, j);
-    txz = tau_in(P, TXZ, i, j);
-    if (!in_stencil(P, i, j)) return;
-    const float* vx = P.in[VX];
-    const float* vz = P.in[VZ];
-    float dvxdx = 0.f, dvzdz = 0.f, dvxdz = 0.f, dvzdx = 0.f;
-#pragma unroll 1
-    for (int l = 1; l <= P.M; ++l) {
-        const float al = P.a[l - 1];
-        dvxdx = fadd(fmul(al, fsub(__ldg(vx + cell(P, i + l, j)), __ldg(vx + cell(P, i - l + 1, j)))), dvxdx);
-        dvzdz = fadd(fmul(al, fsub(__ldg(vz + cell(P, i, j + l - 1)), __ldg(vz + cell(P, i, j - l)))), dvzdz);
-        dvxdz = fadd(fmul(al, fsub(__ldg(vx + cell(P, i, j + l)), __ldg(vx + cell(P, i, j - l + 1)))), dvxdz);
-        dvzdx = fadd(fmul(al, fsub(__ldg(vz + cell(P, i + l - 1, j)), __ldg(vz + cell(P, i - l, j)))), dvzdx);
-    }
-    const size_t c = cell(P, i, j);
-    const float lv = __ldg(P.lam + c), mv = __ldg(P.mu_txx + c), mxz = __ldg(P.mu_txz + c);
-    const float l2m = fadd(lv, fmul(2.f, mv));
-    const float ex = fmul(dvxdx, P.dtx), ez = fmul(dvzdz, P.dtz);
-    txx = fadd(txx, fadd(fmul(l2m, ex), fmul(lv, ez)));
-    tzz = fadd(tzz, fadd(fmul(lv, ex), fmul(l2m, ez)));
-    txz = fadd(txz, fmul(mxz, fadd(fmul(dvxdz, P.dtz), fmul(dvzdx, P.dtx))));
 }
 
 // ---------------------------------------------------------------------------

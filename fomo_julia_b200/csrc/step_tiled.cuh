@@ -203,7 +203,7 @@ __device__ __forceinline__ bool lr_band_cell(const StepParams& P, int i, int j) 
 // into `sin` (field-major, row-major), zero outside the grid.  Velocity:
 // txx, tzz, txz with the source injected; stress: vx, vz.
 template <int M, bool VEL>
-__device__ void load_region_inputs(const StepParams& P, int xa, int za, int W, int H, float* sin) {
+__device__ void load_region_inputs(const StepParams& P, int xa, int za, int W, int H, float* sin, float src_w) {
     const int IW = W + 2 * M, IH = H + 2 * M;
     constexpr int NF = VEL ? 3 : 2;
     const int n = NF * IW * IH;
@@ -213,7 +213,7 @@ __device__ void load_region_inputs(const StepParams& P, int xa, int za, int W, i
         const int i = xa - M + xx, j = za - M + zz;
         float v = 0.f;
         if (i >= 0 && i < P.nx && j >= 0 && j < P.nz)
-            v = VEL ? tau_in(P, TXX + f, i, j) : __ldg(in_field(P, VX + f) + cell(P, i, j));
+            v = VEL ? tau_in(P, TXX + f, i, j, src_w) : __ldg(in_field(P, VX + f) + cell(P, i, j));
         sin[idx] = v;
     }
 }
@@ -222,7 +222,7 @@ __device__ void load_region_inputs(const StepParams& P, int xa, int za, int W, i
 // output fields over [xa, xa+W) x [za, za+H) into `spre` (field-major).
 template <int M, bool VEL>
 __device__ void compute_region_pre(const StepParams& P, const TiledArgs& T, int xa, int za, int W, int H,
-                                   const float* sin, float* spre) {
+                                   const float* sin, float* spre, float src_w) {
     const int IW = W + 2 * M, IH = H + 2 * M;
     auto S = [&](int f, int i, int j) -> float { return sin[(f * IH + (j - za + M)) * IW + (i - xa + M)]; };
     for (int idx = threadIdx.x; idx < W * H; idx += blockDim.x) {
@@ -253,7 +253,7 @@ __device__ void compute_region_pre(const StepParams& P, const TiledArgs& T, int 
             spre[idx] = vx;
             spre[W * H + idx] = vz;
         } else {
-            float txx = tau_in(P, TXX, i, j), tzz = tau_in(P, TZZ, i, j), txz = __ldg(P.in[TXZ] + c);
+            float txx = tau_in(P, TXX, i, j, src_w), tzz = tau_in(P, TZZ, i, j, src_w), txz = __ldg(P.in[TXZ] + c);
             if (in_stencil(P, i, j)) {
                 float dvxdx = 0.f, dvzdz = 0.f, dvxdz = 0.f, dvzdx = 0.f;
 #pragma unroll
@@ -287,14 +287,15 @@ struct SmemPre {
 
 // ---------------------------------------------------------------- edge tiles
 template <int M, bool VEL>
-__device__ void edge_tile(const StepParams& P, const TiledArgs& T, int x0, int z0, int x_end, float* smem) {
+__device__ void edge_tile(const StepParams& P, const TiledArgs& T, int x0, int z0, int x_end, float* smem,
+                          float src_w) {
     using G = Geo<M>;
     const int xa = x0 - kEdgeX, za = z0 - kEdgeZ;
     float* sin = smem;
     float* spre = smem + (VEL ? 3 : 2) * (G::RW + 2 * M) * (G::RH + 2 * M);
-    load_region_inputs<M, VEL>(P, xa, za, G::RW, G::RH, sin);
+    load_region_inputs<M, VEL>(P, xa, za, G::RW, G::RH, sin, src_w);
     __syncthreads();
-    compute_region_pre<M, VEL>(P, T, xa, za, G::RW, G::RH, sin, spre);
+    compute_region_pre<M, VEL>(P, T, xa, za, G::RW, G::RH, sin, spre, src_w);
     __syncthreads();
     for (int idx = threadIdx.x; idx < kTX * kTZ; idx += blockDim.x) {
         const int i = x0 + (idx % kTX), j = z0 + (idx / kTX);
@@ -384,7 +385,7 @@ struct TilePre {
 
 template <int M>
 __device__ __forceinline__ void fast_vel(const StepParams& P, const TiledArgs& T, const VelMapRefs& mp, int x0, int z0,
-                                         int x_end, bool band, bool rim, float* smem) {
+                                         int x_end, bool band, bool rim, float* smem, float src_w) {
     using G = Geo<M>;
     constexpr int BOX = G::BOXS;
     float* s_xx = smem;
@@ -420,8 +421,8 @@ __device__ __forceinline__ void fast_vel(const StepParams& P, const TiledArgs& T
     if (threadIdx.x == 0) {
         const int si = P.src_i - (x0 - G::HX), sj = P.src_j - (z0 - M);
         if (si >= 0 && si < G::BOXW && sj >= 0 && sj < G::BOXH) {
-            s_xx[sj * G::BOXW + si] = fadd(s_xx[sj * G::BOXW + si], P.src_w);
-            s_zz[sj * G::BOXW + si] = fadd(s_zz[sj * G::BOXW + si], P.src_w);
+            s_xx[sj * G::BOXW + si] = fadd(s_xx[sj * G::BOXW + si], src_w);
+            s_zz[sj * G::BOXW + si] = fadd(s_zz[sj * G::BOXW + si], src_w);
         }
     }
     __syncthreads();
@@ -503,7 +504,7 @@ __device__ __forceinline__ void fast_vel(const StepParams& P, const TiledArgs& T
 
 template <int M>
 __device__ __forceinline__ void fast_str(const StepParams& P, const TiledArgs& T, const StrMapRefs& mp, int x0, int z0,
-                                         int x_end, bool band, bool rim, float* smem) {
+                                         int x_end, bool band, bool rim, float* smem, float src_w) {
     using G = Geo<M>;
     constexpr int BOX = G::BOXS;
     float* s_vx = smem;
@@ -565,8 +566,8 @@ __device__ __forceinline__ void fast_str(const StepParams& P, const TiledArgs& T
         const float4 txz = lds4(p_xz + po), lam = lds4(p_lam + po), mu = lds4(p_mu + po), mxz = lds4(p_mxz + po);
         const int dc = P.src_i - x;
         if (zt + rr == P.src_j && dc >= 0 && dc < 4) {
-            set_comp(txx, dc, fadd(comp(txx, dc), P.src_w));
-            set_comp(tzz, dc, fadd(comp(tzz, dc), P.src_w));
+            set_comp(txx, dc, fadd(comp(txx, dc), src_w));
+            set_comp(tzz, dc, fadd(comp(tzz, dc), src_w));
         }
         float2 r_xx[2], r_zz[2], r_xz[2];
 #pragma unroll
@@ -659,15 +660,16 @@ __device__ __forceinline__ TileKind classify(const StepParams& P, const TiledArg
 }
 
 // ---------------------------------------------------------------- receivers
-__device__ inline void record_block(const StepParams& P, int rblock) {
+// rec_k: 1-based step recorded from P.in (P.rec_k on the single-shot path).
+__device__ inline void record_block(const StepParams& P, int rblock, int rec_k) {
     const int r = rblock * blockDim.x + threadIdx.x;
-    if (r >= P.n_rec || P.rec_k < 1) return;
+    if (r >= P.n_rec || rec_k < 1) return;
     const int c = P.rec_cell[r];
     float v;
     if (P.rec_kind == 0) v = P.in[VZ][c];
     else if (P.rec_kind == 1) v = P.in[VX][c];
     else v = fmul(fadd(P.in[TXX][c], P.in[TZZ][c]), 0.5f);
-    P.gather[(size_t)(P.rec_k - 1) + (size_t)r * P.nt] = v;
+    P.gather[(size_t)(rec_k - 1) + (size_t)r * P.nt] = v;
 }
 
 // ---------------------------------------------------------------- kernels
@@ -678,11 +680,11 @@ __global__ void __launch_bounds__(kThreads, 5) velocity_kernel(const __grid_cons
     const int bid = blockIdx.x;
     if (bid < T.n_tile_blocks) {
         const TileKind k = classify(P, T, bid);
-        if (k.generic) edge_tile<M, true>(P, T, k.x0, k.z0, k.x_end, smem);
-        else fast_vel<M>(P, T, refs_of(maps), k.x0, k.z0, k.x_end, k.band, k.rim, smem);
+        if (k.generic) edge_tile<M, true>(P, T, k.x0, k.z0, k.x_end, smem, P.src_w);
+        else fast_vel<M>(P, T, refs_of(maps), k.x0, k.z0, k.x_end, k.band, k.rim, smem, P.src_w);
         return;
     }
-    record_block(P, bid - T.n_tile_blocks);
+    record_block(P, bid - T.n_tile_blocks, P.rec_k);
 }
 
 template <int M>
@@ -692,13 +694,13 @@ __global__ void __launch_bounds__(kThreads, 5) stress_kernel(const __grid_consta
     const int bid = blockIdx.x;
     if (bid < T.n_tile_blocks) {
         const TileKind k = classify(P, T, bid);
-        if (k.generic) edge_tile<M, false>(P, T, k.x0, k.z0, k.x_end, smem);
-        else fast_str<M>(P, T, refs_of(maps), k.x0, k.z0, k.x_end, k.band, k.rim, smem);
+        if (k.generic) edge_tile<M, false>(P, T, k.x0, k.z0, k.x_end, smem, P.src_w);
+        else fast_str<M>(P, T, refs_of(maps), k.x0, k.z0, k.x_end, k.band, k.rim, smem, P.src_w);
     }
 }
 
 // Receivers of the last step (the velocity launch of step k records k-1).
-__global__ void record_kernel(const StepParams P) { record_block(P, blockIdx.x); }
+__global__ void record_kernel(const StepParams P) { record_block(P, blockIdx.x, P.rec_k); }
 
 // ---------------------------------------------------------------- bottom band
 // Rows nz-nbc-1 .. nz-2: the bottom edge and the two bottom corners, whose

@@ -51,6 +51,7 @@ def parse():
     p.add_argument("--no-serving", action="store_true", help="skip the serving section")
     p.add_argument("--batch-nt", type=int, default=None, help="override nt of the batched section (development)")
     p.add_argument("--serve-requests", type=int, default=24)
+    p.add_argument("--no-uneven", action="store_true", help="skip the uneven-batch section")
     return p.parse_args()
 
 
@@ -248,6 +249,62 @@ def batched_section(args):
     }
 
 
+def uneven_section(args):
+    """The uneven batch: 48 shots over four media (600x300, 1200x500,
+    2400x1000, 3200x1400; dx 10 m) with FD orders 4, 8 and 12, nt ~
+    U[1500, 6000] (dt 0.8 ms), 100..800 receivers, 8..15 Hz sources,
+    submitted at once to one ShotServer.  Sequential plain time per shot is
+    its (medium, order)'s measured single-shot device step time times nt."""
+    import fomo_julia_b200 as F
+    from fomo_julia_b200 import synthetic
+    B = F.backend("b200")
+    dt = 0.0008
+    reqs = synthetic.uneven_requests()
+    base = synthetic.uneven_media()
+    med, hab = {}, {}
+    for m, order in sorted({(q.medium, q.fd_order) for q in reqs}):
+        (vp, vs, rho), dx = base[m]
+        M = F.init_medium(vp, vs, rho, dx, dx, 50, order, B, free_surface=True)
+        med[(m, order)] = M
+        hab[(m, order)] = F.init_habc(M.nx, M.nz, 50, dt, dx, dx, F.julia_mean(vp), B)
+    plain_step = {}
+    for key, M in med.items():
+        W = F.Wavefield(M.nx, M.nz, B)
+        a = F.get_fd_coefficients(key[1])
+        src = F.Source(M.nx // 2, M.pad + 2, F.ricker_wavelet(10.0, dt, 200))
+        rec = F.setup_receivers(np.linspace(0, (M.nx - 2 * M.pad - 1) * M.dx, 400).astype(np.float32),
+                                np.full(400, 10.0, np.float32), M)
+        F.run_shot(B, W, M, hab[key], a, src, rec, F.sim_params(dt, 200, M.dx, M.dz, key[1]))
+        r = F.run_shot(B, W, M, hab[key], a, src, rec, F.sim_params(dt, 200, M.dx, M.dz, key[1]))
+        plain_step[key] = r.stats["device_ms"] / 1e3 / 200
+        W.release()
+    plain_total = sum(plain_step[(q.medium, q.fd_order)] * q.nt for q in reqs)
+    with F.ShotServer() as srv:
+        t0 = time.perf_counter()
+        ts = []
+        for k, q in enumerate(reqs):
+            M = med[(q.medium, q.fd_order)]
+            nx_in = M.nx - 2 * M.pad
+            src = F.Source(F.coord_to_index(q.src_x, M.dx, M.pad), F.coord_to_index(q.src_z, M.dz, M.pad),
+                           F.ricker_wavelet(q.f0, dt, q.nt))
+            rec = F.setup_receivers(np.linspace(0, (nx_in - 1) * M.dx, q.n_rec).astype(np.float32),
+                                    np.full(q.n_rec, 10.0, np.float32), M)
+            ts.append(srv.submit(M, hab[(q.medium, q.fd_order)], F.get_fd_coefficients(q.fd_order), src, rec,
+                                 F.sim_params(dt, q.nt, M.dx, M.dz, q.fd_order), k))
+        srv.wait_all(ts)
+        makespan = time.perf_counter() - t0
+        st = srv.stats()
+    for M in med.values():
+        M.release()
+    cell_steps = sum(med[(q.medium, q.fd_order)].nx * med[(q.medium, q.fd_order)].nz * q.nt for q in reqs)
+    return {"shots": len(reqs), "media_orders": len(med), "makespan_s": makespan,
+            "batched_shots_per_hour": len(reqs) * 3600.0 / makespan,
+            "plain_shots_per_hour": len(reqs) * 3600.0 / plain_total,
+            "speedup_vs_plain": plain_total / makespan, "batched_gcell_steps_s": cell_steps / makespan / 1e9,
+            "plain": "device step time of one shot per (medium, order) x nt, shots one after another",
+            "peak_shots": st["peak_shots"], "kernel_launches": st["kernel_launches"]}
+
+
 def serving_section(args, c1):
     """A Poisson stream of shot requests over six resident media (600x300,
     1200x500, 2400x1000, 3200x1400, 2000x800 and the 4444x3819 medium),
@@ -400,10 +457,20 @@ def b200_arm(args, rank, world, local):
         call("fomo_b200_shot_finish", sh.value, None, ctypes.byref(st))
         return st
 
+    model = []
+    for arr in (w.vp, w.vs, w.rho):
+        t = torch.empty(arr.size, dtype=torch.float32, pin_memory=True)
+        t.numpy()[:] = np.asfortranarray(arr).ravel(order="F")
+        model.append(t)
+
     def e2e_shot():
-        """The drop-in call sequence with host buffers: upload the medium,
-        run the shot, read the gather back, release the medium."""
-        m2 = medium_create()
+        """The drop-in call sequence with host buffers: create the medium
+        from the unpadded model (padding and staggered parameters on the
+        device), run the shot, read the gather back, release the medium."""
+        h = ctypes.c_uint64(0)
+        call("fomo_b200_medium_create_from_model", w.nx_in, w.nz_in, *[t.data_ptr() for t in model], float(w.dx),
+             float(w.dz), w.nbc, w.fd_order // 2, int(w.free_surface), ctypes.byref(h))
+        m2 = h.value
         st = FomoRunStats()
         call("fomo_b200_run_shot", m2, wf, ctypes.byref(H), ctypes.byref(S), gather.data_ptr(), ctypes.byref(st))
         call("fomo_b200_medium_destroy", m2)
@@ -448,13 +515,14 @@ def b200_arm(args, rank, world, local):
         e2e_shot()
         with ClockSampler(local) as clk_e:
             ms_e, _, st_e = timed(e2e_shot, args.steps)
-        h2d = sum(t.numel() * 4 for t in pinned) + st_e[0].h2d_bytes
+        h2d = sum(t.numel() * 4 for t in model) + st_e[0].h2d_bytes
         e2e = {"value": world * args.steps * cells * w.nt / (ms_e / 1e3) / 1e9, "unit": METRIC,
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(st_e[0].d2h_bytes),
                "ms_per_step": ms_e / args.steps,
                "loop_ms_per_shot": [round(t.device_ms, 2) for t in st_e],
                "clocks": clk_e.summary(),
-               "path": "fomo_b200_medium_create + fomo_b200_run_shot (pinned host buffers) + medium_destroy"}
+               "path": "fomo_b200_medium_create_from_model (unpadded vp/vs/rho from pinned host memory) + "
+                       "fomo_b200_run_shot (gather to pinned host memory) + fomo_b200_medium_destroy"}
 
     # roofline of the dominant kernel: CUDA events around each launch
     sh = ctypes.c_uint64(0)
@@ -501,12 +569,14 @@ def b200_arm(args, rank, world, local):
                "sample": f"first {n} time steps of the same shot ({t:.1f} s), C++ restatement of the "
                          f"reference's Float32 CPU path (oracle/), OpenMP"}
 
-    batched = served = None
+    batched = served = uneven = None
     if rank == 0 and world == 1:
         call("fomo_b200_wavefield_destroy", wf)
         wf = None
         if not args.no_batched:
             batched = batched_section(args)
+        if not args.no_uneven:
+            uneven = uneven_section(args)
         if not args.no_serving:
             pad = hi["pad"]
             c1_medium = F.Medium(nx, nz, float(w.dx), float(w.dz), 0.0, 0.0, w.fd_order // 2, pad,
@@ -527,7 +597,7 @@ def b200_arm(args, rank, world, local):
             "loop_ms_per_shot": [round(t.device_ms, 2) for t in st_v],
             "e2e": e2e, "gpu_launches": int(launches), "clocks": clocks, "roofline": roofline,
             "cpu_baseline": cpu,
-            "batched": batched, "serving": served,
+            "batched": batched, "uneven": uneven, "serving": served,
         }
         print(json.dumps(line), flush=True)
     if world > 1:

@@ -6,6 +6,7 @@
 #include <cuda.h>
 #include <cudaTypedefs.h>
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <algorithm>
 #include <atomic>
@@ -358,6 +359,7 @@ int run_steps_M(Shot& s, Medium& m, Wavefield& w, int n_steps, Profile* prof) {
     const int rec_blocks = (s.n_rec + fomo::kThreads - 1) / fomo::kThreads;
     CUDA_TRY(cudaEventRecord(C.ev0, C.stream));
     const int k_end = std::min(s.nt, s.k_done + n_steps);
+    nvtxRangePushA("fomo_b200 time loop");
     for (int k = s.k_done + 1; k <= k_end; ++k) {
         const int a = w.cur, b = 1 - w.cur;
         fomo::StepParams P;
@@ -411,6 +413,7 @@ int run_steps_M(Shot& s, Medium& m, Wavefield& w, int n_steps, Profile* prof) {
         if (k >= 2) s.recorded = k - 1;
         s.k_done = k;
     }
+    nvtxRangePop();
     CUDA_TRY(cudaGetLastError());
     CUDA_TRY(cudaEventRecord(C.ev1, C.stream));
     CUDA_TRY(cudaEventSynchronize(C.ev1));
@@ -922,6 +925,21 @@ int fomo_b200_shot_profile(uint64_t shot_handle, int32_t n_steps, FomoKernelTime
         out[prof.kind[i]].total_ms += ms;
     }
     *n_kinds = 4;
+    return FOMO_OK;
+}
+
+int fomo_b200_selftest_wait(int32_t polls, int32_t* status) {
+    std::lock_guard<std::mutex> lk(ctx().mu);
+    if (int rc = ensure_init()) return rc;
+    if (polls < 1 || polls > (1 << 20) || !status) return fail(FOMO_EINVAL, "polls must be 1..2^20");
+    cudaStream_t st = ctx().stream;
+    CUDA_TRY(cudaMemsetAsync(ctx().d_status, 0, sizeof(int), st));
+    fomo::wait_selftest_kernel<<<1, 32, 0, st>>>(ctx().d_status, polls);
+    CUDA_TRY(cudaGetLastError());
+    const int rc = check_status();
+    *status = rc;
+    CUDA_TRY(cudaMemsetAsync(ctx().d_status, 0, sizeof(int), st));
+    CUDA_TRY(cudaStreamSynchronize(st));
     return FOMO_OK;
 }
 

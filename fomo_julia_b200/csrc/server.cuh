@@ -21,6 +21,8 @@
 #pragma once
 
 #include <chrono>
+#include <cstdio>
+#include <cstdlib>
 #include <condition_variable>
 #include <deque>
 #include <map>
@@ -131,6 +133,35 @@ struct TuneEntry {
 std::mutex g_tune_mu;
 std::map<TuneKey, TuneEntry> g_tune;  // process-wide cache: (grid, order, batch size) -> K
 
+// Optional file behind the cache (environment variable FOMO_B200_TUNE_CACHE):
+// one line "nx nz M shots_log2 K" per decision, read when a server starts and
+// appended to when a choice is made.  Call with g_tune_mu held.
+const char* tune_cache_path() {
+    const char* p = std::getenv("FOMO_B200_TUNE_CACHE");
+    return (p && *p) ? p : nullptr;
+}
+
+void load_tune_cache() {
+    const char* path = tune_cache_path();
+    if (!path) return;
+    FILE* f = std::fopen(path, "r");
+    if (!f) return;
+    int nx, nz, M, lg, K;
+    while (std::fscanf(f, "%d %d %d %d %d", &nx, &nz, &M, &lg, &K) == 5)
+        for (int c = 0; c < 3; ++c)
+            if (kTuneK[c] == K) g_tune[TuneKey{nx, nz, M, lg}].chosen = c;
+    std::fclose(f);
+}
+
+void save_tune_choice(const TuneKey& k, int cand) {
+    const char* path = tune_cache_path();
+    if (!path) return;
+    if (FILE* f = std::fopen(path, "a")) {
+        std::fprintf(f, "%d %d %d %d %d\n", k.nx, k.nz, k.M, k.shots_log2, kTuneK[cand]);
+        std::fclose(f);
+    }
+}
+
 // Largest dynamic shared memory set so far for the batch kernels, per M.
 std::mutex g_batch_attr_mu;
 size_t g_batch_smem[2][fomo::kMaxM + 1] = {};
@@ -229,6 +260,10 @@ class Server {
             budget_ = (size_t)(0.9 * (double)fr);
         } else {
             budget_ = cfg_.hbm_budget_bytes;
+        }
+        {
+            std::lock_guard<std::mutex> lk(g_tune_mu);
+            load_tune_cache();
         }
         worker_ = std::thread([this] { loop(); });
         return FOMO_OK;
@@ -818,7 +853,10 @@ class Server {
                     if (e.ms_per_step[c] < 0) all = false;
                     else if (e.ms_per_step[best] < 0 || e.ms_per_step[c] < e.ms_per_step[best]) best = c;
                 }
-                if (all && e.chosen < 0) e.chosen = best;
+                if (all && e.chosen < 0) {
+                    e.chosen = best;
+                    save_tune_choice(m.key, best);
+                }
             }
             release_event(m.a, true);
             release_event(m.b, true);
@@ -849,10 +887,14 @@ class Server {
             ms.b = event(true);
             CUDA_TRY(cudaEventRecord(ms.a, st_));
         }
+        nvtxRangePushA(graph ? "fomo_b200 batch graph replay" : "fomo_b200 batch launches");
         if (graph) {
-            CUDA_TRY(cudaGraphLaunch(x, st_));
+            const cudaError_t e = cudaGraphLaunch(x, st_);
+            nvtxRangePop();
+            CUDA_TRY(e);
         } else {
             for (int k = 0; k < n; ++k) enqueue_step();
+            nvtxRangePop();
             CUDA_TRY(cudaGetLastError());
         }
         if (measure) {

@@ -167,12 +167,32 @@ __device__ __forceinline__ void set_comp(float4& v, int c, float x) {
     if (c == 0) v.x = x; else if (c == 1) v.y = x; else if (c == 2) v.z = x; else v.w = x;
 }
 
+// Bounded wait on phase 0 of an mbarrier: false (and kErrTmaTimeout in the
+// status word) after `limit` unsuccessful polls, so a load that never lands
+// ends the block with an error the host reads instead of hanging the GPU.
+constexpr int kWaitPolls = 1 << 24;
+__device__ __forceinline__ bool bounded_wait(uint64_t* bar, int* status, int limit) {
+    for (int it = 0; it < limit; ++it)
+        if (mbar_try_wait(bar, 0)) return true;
+    atomicCAS(status, 0, kErrTmaTimeout);
+    return false;
+}
+
 // Waits for the TMA boxes of this block; false (and status set) on timeout.
 __device__ __forceinline__ bool wait_tma(uint64_t* bar, const TiledArgs& T) {
-    for (int it = 0; it < (1 << 24); ++it)
-        if (mbar_try_wait(bar, 0)) return true;
-    atomicCAS(T.status, 0, kErrTmaTimeout);
-    return false;
+    return bounded_wait(bar, T.status, kWaitPolls);
+}
+
+// Self-test of the bounded wait: thread 0 arms an mbarrier for a byte count
+// that no copy delivers and waits `limit` polls on it, exactly as a tile
+// waits for its TMA boxes; no memory operation is outstanding.
+__global__ void wait_selftest_kernel(int* status, int limit) {
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x != 0) return;
+    mbar_init(&bar, 1);
+    fence_barrier_init();
+    mbar_expect_tx(&bar, 16);
+    bounded_wait(&bar, status, limit);
 }
 
 // Rows a tile stores: every row of the grid.  Rows nz-nbc-1 .. nz-2 (the

@@ -230,6 +230,15 @@ typedef struct {
 int fomo_b200_shot_profile(uint64_t shot_handle, int32_t n_steps, FomoKernelTime* out,
                            int32_t max_kinds, int32_t* n_kinds);
 
+/* Self-test of the kernels' bounded device waits (no reference
+ * counterpart).  Every wait of a time-step kernel on its TMA loads polls at
+ * most a fixed number of times, then records an error that the call reports
+ * as FOMO_ETIMEOUT instead of hanging the GPU.  This runs the same wait on a
+ * barrier that nothing completes, for `polls` polls (1..2^20), and stores
+ * the resulting status in *status (FOMO_ETIMEOUT when the mechanism works);
+ * nothing is left outstanding on the device. */
+int fomo_b200_selftest_wait(int32_t polls, int32_t* status);
+
 /* Allocation-free shot.  No counterpart in the reference: it exists for
  * callers that cannot allocate device memory while a shot runs -- a caller
  * capturing its stream into a CUDA graph (allocation cannot be captured), a

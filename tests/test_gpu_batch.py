@@ -223,3 +223,55 @@ def test_more_media_than_one_launch_holds(b200):
         assert np.array_equal(r.gather, g)
     for S in Ss:
         S.med.release()
+
+
+def test_bounded_device_wait_reports_timeout(b200):
+    """The kernels' bounded wait, run on a barrier nothing completes, ends
+    with FOMO_ETIMEOUT and leaves the context usable."""
+    import ctypes
+    from fomo_julia_b200._lib import call
+    st = ctypes.c_int32(0)
+    call("fomo_b200_selftest_wait", 1000, ctypes.byref(st))
+    assert st.value == -4
+    c = layered(41, 27, seed=3, nbc=7, fd_order=8, nt=50)
+    S = setup(c, b200)
+    g = single(S, source(S, 100.0, 20.0), b200)
+    assert np.isfinite(g).all() and np.abs(g).max() > 0
+    S.med.release()
+
+
+def test_server_rejects_bad_requests(b200):
+    import ctypes
+    from fomo_julia_b200._lib import FomoHabc, FomoShot, call
+    c = layered(41, 27, seed=3, nbc=7, fd_order=8, nt=50)
+    S = setup(c, b200)
+    with F.ShotServer() as srv:
+        t = ctypes.c_uint64(0)
+        with pytest.raises(FomoError) as e:  # a medium handle that does not exist
+            call("fomo_b200_server_submit", srv.handle, 987654, ctypes.byref(FomoHabc()), ctypes.byref(FomoShot()),
+                 None, ctypes.byref(t))
+        assert e.value.code == -1
+        bad = layered(41, 27, seed=3, nbc=7, fd_order=8, nt=50)
+        bad.src_x = 1.0e6  # source outside the grid
+        with pytest.raises(FomoError):
+            srv.submit(S.med, S.H, S.a, source(S, bad.src_x, 20.0), S.rec, params_of(S))
+        with pytest.raises(FomoError):
+            srv.wait(F.Ticket(424242, 0, None, None, None))
+        ok = srv.wait(srv.submit(S.med, S.H, S.a, source(S, 100.0, 20.0), S.rec, params_of(S)), timeout=WAIT_S)
+        assert ok.stats["steps"] == 50
+    with pytest.raises(FomoError):
+        call("fomo_b200_server_destroy", 987654)
+    S.med.release()
+
+
+def test_tune_cache_file(b200, tmp_path, monkeypatch):
+    path = tmp_path / "tune.txt"
+    monkeypatch.setenv("FOMO_B200_TUNE_CACHE", str(path))
+    c = layered(97, 61, seed=8, nbc=6, fd_order=8, nt=400)
+    S = setup(c, b200)
+    with F.ShotServer() as srv:  # autotuned K: the three candidates are measured on live chunks
+        srv.wait_all([srv.submit(S.med, S.H, S.a, source(S, 100.0 + 30 * k, 20.0), S.rec, params_of(S))
+                      for k in range(3)], timeout=WAIT_S)
+    lines = path.read_text().split("\n")
+    assert any(l.startswith(f"{S.med.nx} {S.med.nz} 4 1 ") for l in lines), lines
+    S.med.release()

@@ -50,7 +50,7 @@ def parse():
     p.add_argument("--no-batched", action="store_true", help="skip the batched-shots section")
     p.add_argument("--no-serving", action="store_true", help="skip the serving section")
     p.add_argument("--batch-nt", type=int, default=None, help="override nt of the batched section (development)")
-    p.add_argument("--serve-requests", type=int, default=24)
+    p.add_argument("--serve-requests", type=int, default=48)
     p.add_argument("--no-uneven", action="store_true", help="skip the uneven-batch section")
     return p.parse_args()
 

@@ -259,15 +259,15 @@ struct Launch {
 };
 
 template <int M>
-Launch launch_shape(int nx, int nz, int nbc, bool iso) {
+Launch launch_shape(int nx, int nz, int nbc, bool iso, bool fs) {
     Launch L;
     L.tiles_x = (nx + fomo::kTX - 1) / fomo::kTX;
     L.tiles_z = (nz + fomo::kTZ - 1) / fomo::kTZ;
     L.x_last = std::max(0, (nx + 3) / 4 * 4 - fomo::kTX);  // last tile ends at the grid's right edge
     L.n_tile = L.tiles_x * L.tiles_z;
     L.n_band = fomo::band_warp_count(nx);
-    L.smem_v = fomo::tiled_smem_bytes<M>(true, nbc, iso);
-    L.smem_s = fomo::tiled_smem_bytes<M>(false, nbc, iso);
+    L.smem_v = fomo::tiled_smem_bytes<M>(true, nbc, iso, fs);
+    L.smem_s = fomo::tiled_smem_bytes<M>(false, nbc, iso, fs);
     return L;
 }
 
@@ -334,7 +334,7 @@ template <int M>
 int run_steps_M(Shot& s, Medium& m, Wavefield& w, int n_steps, Profile* prof) {
     auto& C = ctx();
     const bool iso = s.dtx == s.dtz;
-    const Launch L = launch_shape<M>(m.nx, m.nz, s.nbc, iso);
+    const Launch L = launch_shape<M>(m.nx, m.nz, s.nbc, iso, m.fs != 0);
     static size_t smem_set_v = 48 * 1024, smem_set_s = 48 * 1024;
     if (L.smem_v > smem_set_v) {
         CUDA_TRY(cudaFuncSetAttribute(fomo::velocity_kernel<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.smem_v));
@@ -1025,7 +1025,7 @@ int noalloc_loop(const fomo::StepParams& P0, fomo::TiledArgs T, float* fields, i
         if (int rc = encode_map(&mod[q], med[2 + q], nx, nz, pitch, fomo::kTX, fomo::kTZ)) return rc;
     for (int q = 0; q < 4; ++q)
         if (int rc = encode_map(&bm[q], buoy[q], nx, nz, pitch, fomo::kTX, fomo::kTZ)) return rc;
-    const Launch L = launch_shape<M>(nx, nz, P0.nbc, iso);
+    const Launch L = launch_shape<M>(nx, nz, P0.nbc, iso, P0.fs != 0);
     if (L.smem_v > 48 * 1024)
         CUDA_TRY(cudaFuncSetAttribute(fomo::velocity_kernel<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.smem_v));
     if (L.smem_s > 48 * 1024)

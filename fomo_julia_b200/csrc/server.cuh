@@ -166,14 +166,14 @@ void save_tune_choice(const TuneKey& k, int cand) {
 std::mutex g_batch_attr_mu;
 size_t g_batch_smem[2][fomo::kMaxM + 1] = {};
 
-size_t batch_smem_any(int M, bool vel, int nbc, bool iso) {
+size_t batch_smem_any(int M, bool vel, int nbc, bool iso, bool fs) {
     switch (M) {
-        case 1: return fomo::tiled_smem_bytes<1>(vel, nbc, iso);
-        case 2: return fomo::tiled_smem_bytes<2>(vel, nbc, iso);
-        case 3: return fomo::tiled_smem_bytes<3>(vel, nbc, iso);
-        case 4: return fomo::tiled_smem_bytes<4>(vel, nbc, iso);
-        case 5: return fomo::tiled_smem_bytes<5>(vel, nbc, iso);
-        case 6: return fomo::tiled_smem_bytes<6>(vel, nbc, iso);
+        case 1: return fomo::tiled_smem_bytes<1>(vel, nbc, iso, fs);
+        case 2: return fomo::tiled_smem_bytes<2>(vel, nbc, iso, fs);
+        case 3: return fomo::tiled_smem_bytes<3>(vel, nbc, iso, fs);
+        case 4: return fomo::tiled_smem_bytes<4>(vel, nbc, iso, fs);
+        case 5: return fomo::tiled_smem_bytes<5>(vel, nbc, iso, fs);
+        case 6: return fomo::tiled_smem_bytes<6>(vel, nbc, iso, fs);
     }
     return 0;
 }
@@ -557,8 +557,8 @@ class Server {
         L.n_tile = L.tiles_x * L.tiles_z;
         L.n_band = fomo::band_warp_count(m.nx);
         const bool iso = r.dtx == r.dtz;
-        L.smem_v = batch_smem_any(r.M, true, r.nbc, iso);
-        L.smem_s = batch_smem_any(r.M, false, r.nbc, iso);
+        L.smem_v = batch_smem_any(r.M, true, r.nbc, iso, m.fs != 0);
+        L.smem_s = batch_smem_any(r.M, false, r.nbc, iso, m.fs != 0);
         return L;
     }
 
@@ -1168,7 +1168,7 @@ int make_request(Medium* m, const FomoHabc* habc, const FomoShot* shot, float* g
     if (shot->rec_kind < 0 || shot->rec_kind > 2) return fail(FOMO_EINVAL, "bad receiver kind %d", shot->rec_kind);
     if (shot->n_rec > 0 && shot->nt > 0 && !gather_out) return fail(FOMO_EINVAL, "gather_out is NULL");
     const bool iso = shot->dtx == shot->dtz;
-    const size_t smem = std::max(batch_smem_any(m->M, true, nbc, iso), batch_smem_any(m->M, false, nbc, iso));
+    const size_t smem = std::max(batch_smem_any(m->M, true, nbc, iso, m->fs != 0), batch_smem_any(m->M, false, nbc, iso, m->fs != 0));
     if (smem > 227 * 1024)
         return fail(FOMO_EINVAL, "nbc=%d needs %zu bytes of shared memory per block, more than 227 KB", nbc, smem);
     auto r = std::make_shared<Request>();

@@ -132,7 +132,7 @@ __device__ __forceinline__ float wavelet_at(const BatchShot& S, int ks) {
 }
 
 template <int M>
-__global__ void __launch_bounds__(kThreads, 5) batch_velocity_kernel(const __grid_constant__ BatchVelLaunch L) {
+__global__ void __launch_bounds__(kThreads, kTileBlocks<M>) batch_velocity_kernel(const __grid_constant__ BatchVelLaunch L) {
     extern __shared__ __align__(128) float smem[];
     const BatchItem it = decode(L.H, blockIdx.x, true, false);
     if (it.role < 0) return;
@@ -158,7 +158,7 @@ __global__ void __launch_bounds__(kThreads, 5) batch_velocity_kernel(const __gri
 }
 
 template <int M>
-__global__ void __launch_bounds__(kThreads, 5) batch_stress_kernel(const __grid_constant__ BatchStrLaunch L) {
+__global__ void __launch_bounds__(kThreads, kTileBlocks<M>) batch_stress_kernel(const __grid_constant__ BatchStrLaunch L) {
     extern __shared__ __align__(128) float smem[];
     const BatchItem it = decode(L.H, blockIdx.x, false, false);
     if (it.role < 0) return;

@@ -37,6 +37,10 @@ namespace fomo {
 
 constexpr int kTX = 64, kTZ = 16, kThreads = 128;
 constexpr int kCG = kTX / 4;   // float4 column groups of a tile row
+// Tile blocks per SM the register allocation is sized for.  Six blocks
+// (80 registers) for M <= 4 were measured no faster than five.
+template <int M>
+constexpr int kTileBlocks = 5;
 constexpr int kStripW = 28;     // columns a band-pass warp stores
 constexpr int kMarchRows = 16;  // band rows staged per chunk by the band pass
 
@@ -694,7 +698,7 @@ __device__ inline void record_block(const StepParams& P, int rblock, int rec_k) 
 
 // ---------------------------------------------------------------- kernels
 template <int M>
-__global__ void __launch_bounds__(kThreads, 5) velocity_kernel(const __grid_constant__ StepParams P, const __grid_constant__ TiledArgs T,
+__global__ void __launch_bounds__(kThreads, kTileBlocks<M>) velocity_kernel(const __grid_constant__ StepParams P, const __grid_constant__ TiledArgs T,
                                                             const __grid_constant__ VelMaps maps) {
     extern __shared__ __align__(128) float smem[];
     const int bid = blockIdx.x;
@@ -708,7 +712,7 @@ __global__ void __launch_bounds__(kThreads, 5) velocity_kernel(const __grid_cons
 }
 
 template <int M>
-__global__ void __launch_bounds__(kThreads, 5) stress_kernel(const __grid_constant__ StepParams P, const __grid_constant__ TiledArgs T,
+__global__ void __launch_bounds__(kThreads, kTileBlocks<M>) stress_kernel(const __grid_constant__ StepParams P, const __grid_constant__ TiledArgs T,
                                                           const __grid_constant__ StrMaps maps) {
     extern __shared__ __align__(128) float smem[];
     const int bid = blockIdx.x;
@@ -911,16 +915,18 @@ __global__ void buoyancy_kernel(const float* rho_vx, const float* rho_vz, float 
     }
 }
 
-// Shared-memory bytes of one launch (the largest block role).
+// Shared-memory bytes of one launch (the largest block role that can occur:
+// generic tiles only without a free surface or with a band wider than a tile
+// allows, as classify decides).
 template <int M>
-__host__ size_t tiled_smem_bytes(bool vel, int nbc, bool iso) {
-    (void)nbc;  // the bottom band runs in its own launch
+__host__ size_t tiled_smem_bytes(bool vel, int nbc, bool iso, bool fs) {
     using G = Geo<M>;
     const int nin = vel ? 3 : 2, nout = vel ? 2 : 3;
     const int npoint = vel ? (iso ? 4 : 6) : 6;
     const size_t interior = ((size_t)nin * G::BOXS + (size_t)npoint * kPBox) * 4 + 16;
     const size_t edge = ((size_t)nin * (G::RW + 2 * M) * (G::RH + 2 * M) + (size_t)nout * G::RW * G::RH) * 4;
-    return std::max(interior, edge);
+    const bool generic = !fs || nbc + 6 > kTX;
+    return generic ? std::max(interior, edge) : interior;
 }
 
 }  // namespace fomo

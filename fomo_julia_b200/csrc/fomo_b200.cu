@@ -14,6 +14,7 @@
 #include <cstdio>
 #include <cstring>
 #include <memory>
+#include <utility>
 #include <mutex>
 #include <string>
 #include <unordered_map>
@@ -104,7 +105,7 @@ struct Shot : Object {
     int nt = 0, src_i = 0, src_j = 0, n_rec = 0, rec_kind = 0;
     std::vector<float> wavelet;     // host copy: one sample per step
     float* d_tabs = nullptr;        // 3 x (nbc+2)
-    float* d_band = nullptr;        // band scratch: 3 planes of nbc rows x pitch
+    float* d_band = nullptr;        // band scratch: kBandPlanes planes of nbc rows x pitch
     int* d_rec = nullptr;           // n_rec linear offsets
     float* d_gather = nullptr;      // nt x n_rec
     int k_done = 0, recorded = 0;
@@ -330,6 +331,26 @@ int check_status() {
     return FOMO_OK;
 }
 
+// Launches a tile kernel.  With `after_band` (the launch just before it on
+// the stream is a band pass) it is a programmatic dependent launch: its
+// blocks start while the band pass runs, and those that read the band rows
+// wait for it (grid_dep_wait).
+template <class... Exp, class... Act>
+static cudaError_t launch_tiles(void (*kern)(Exp...), int blocks, size_t smem, cudaStream_t st, bool after_band,
+                                Act&&... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(blocks);
+    cfg.blockDim = dim3(fomo::kThreads);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = after_band ? 1 : 0;
+    return cudaLaunchKernelEx(&cfg, kern, std::forward<Act>(args)...);
+}
+
 template <int M>
 int run_steps_M(Shot& s, Medium& m, Wavefield& w, int n_steps, Profile* prof) {
     auto& C = ctx();
@@ -358,9 +379,9 @@ int run_steps_M(Shot& s, Medium& m, Wavefield& w, int n_steps, Profile* prof) {
     T.x_last = L.x_last;
     const int rec_blocks = (s.n_rec + fomo::kThreads - 1) / fomo::kThreads;
     CUDA_TRY(cudaEventRecord(C.ev0, C.stream));
-    const int k_end = std::min(s.nt, s.k_done + n_steps);
+    const int k_begin = s.k_done + 1, k_end = std::min(s.nt, s.k_done + n_steps);
     nvtxRangePushA("fomo_b200 time loop");
-    for (int k = s.k_done + 1; k <= k_end; ++k) {
+    for (int k = k_begin; k <= k_end; ++k) {
         const int a = w.cur, b = 1 - w.cur;
         fomo::StepParams P;
         fill_common(P, m, s);
@@ -382,7 +403,8 @@ int run_steps_M(Shot& s, Medium& m, Wavefield& w, int n_steps, Profile* prof) {
         vm.b1 = m.buoy_maps[1];
         vm.b2 = m.buoy_maps[2];
         vm.b3 = m.buoy_maps[3];
-        fomo::velocity_kernel<M><<<vblocks, fomo::kThreads, L.smem_v, C.stream>>>(P, T, vm);
+        // profiled launches stay serialised (events sit between them)
+        CUDA_TRY(launch_tiles(fomo::velocity_kernel<M>, vblocks, L.smem_v, C.stream, !prof && k > k_begin, P, T, vm));
         if (prof && prof->end(C.stream)) return fail(FOMO_ECUDA, "profiling event failed");
         if (prof && prof->add(C.stream, 2)) return fail(FOMO_ECUDA, "profiling event failed");
         fomo::band_kernel<true><<<L.n_band, 32, 0, C.stream>>>(P, T);
@@ -403,7 +425,7 @@ int run_steps_M(Shot& s, Medium& m, Wavefield& w, int n_steps, Profile* prof) {
         sm.lam = m.mod_maps[0];
         sm.mu = m.mod_maps[1];
         sm.mxz = m.mod_maps[2];
-        fomo::stress_kernel<M><<<L.n_tile, fomo::kThreads, L.smem_s, C.stream>>>(P, T, sm);
+        CUDA_TRY(launch_tiles(fomo::stress_kernel<M>, L.n_tile, L.smem_s, C.stream, !prof, P, T, sm));
         if (prof && prof->end(C.stream)) return fail(FOMO_ECUDA, "profiling event failed");
         if (prof && prof->add(C.stream, 3)) return fail(FOMO_ECUDA, "profiling event failed");
         fomo::band_kernel<false><<<L.n_band, 32, 0, C.stream>>>(P, T);
@@ -834,7 +856,7 @@ int fomo_b200_shot_begin(uint64_t medium, uint64_t wavefield, const FomoHabc* ha
     s->rec_kind = shot->rec_kind;
     const size_t tab_n = (size_t)nbc + 2;
     cudaError_t e = cudaMalloc(&s->d_tabs, 3 * tab_n * sizeof(float));
-    if (e == cudaSuccess) e = cudaMalloc(&s->d_band, 3 * (size_t)nbc * m->pitch * sizeof(float));
+    if (e == cudaSuccess) e = cudaMalloc(&s->d_band, fomo::kBandPlanes * (size_t)nbc * m->pitch * sizeof(float));
     if (e == cudaSuccess && s->n_rec) e = cudaMalloc(&s->d_rec, s->n_rec * sizeof(int));
     if (e == cudaSuccess && s->n_rec && s->nt)
         e = cudaMalloc(&s->d_gather, (size_t)s->nt * s->n_rec * sizeof(float));
@@ -1124,7 +1146,7 @@ extern "C" int fomo_b200_run_shot_noalloc(int32_t nx, int32_t nz, int32_t M, int
     const size_t off_rec = off_tab + align256(3 * (size_t)(nbc + 2) * sizeof(float));
     const size_t off_buo = off_rec + align256((size_t)shot->n_rec * sizeof(int));
     const size_t off_band = off_buo + align256((iso ? 2 : 4) * plane);
-    const size_t off_wf = off_band + align256(3 * (size_t)nbc * pitch * sizeof(float));
+    const size_t off_wf = off_band + align256(fomo::kBandPlanes * (size_t)nbc * pitch * sizeof(float));
     const size_t need = off_wf + 10 * plane;
     if (need > kNoAllocScratchBytes)
         return fail(FOMO_EINVAL, "shot needs %zu bytes of scratch, more than the %zu-byte static array of "

@@ -562,8 +562,8 @@ class Server {
         return L;
     }
 
-    // Bytes of a shot's band scratch (three planes of nbc rows).
-    static size_t band_bytes(const Request& r) { return 3 * (size_t)r.nbc * r.med->pitch * sizeof(float); }
+    // Bytes of a shot's band scratch (kBandPlanes planes of nbc rows).
+    static size_t band_bytes(const Request& r) { return fomo::kBandPlanes * (size_t)r.nbc * r.med->pitch * sizeof(float); }
 
     // Bytes of the pinned upload area of a shot.
     static size_t stage_bytes(const Request& r) {
@@ -1203,7 +1203,7 @@ int make_request(Medium* m, const FomoHabc* habc, const FomoShot* shot, float* g
     }
     r->gather_out = gather_out;
     const size_t plane = (size_t)m->pitch * m->nz * sizeof(float);
-    r->bytes = 10 * plane + align_up(3 * (size_t)nbc * m->pitch * sizeof(float), 256) + align_up(r->tabs.size() * 4, 256) + align_up(r->cells.size() * 4, 256) +
+    r->bytes = 10 * plane + align_up(fomo::kBandPlanes * (size_t)nbc * m->pitch * sizeof(float), 256) + align_up(r->tabs.size() * 4, 256) + align_up(r->cells.size() * 4, 256) +
                align_up(std::max<size_t>(r->wavelet.size(), 1) * 4, 256) +
                align_up((size_t)r->nt * r->n_rec * 4, 256);
     r->buoy_bytes = (iso ? 2 : 4) * plane;

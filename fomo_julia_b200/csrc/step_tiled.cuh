@@ -157,6 +157,14 @@ __device__ __forceinline__ void cp_async4(float* dst, const float* src, bool val
                  : "memory");
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+
+// Programmatic dependent launch.  A band pass lets the tile launch that
+// follows it start at once (grid_dep_trigger); a tile block that reads what
+// the band pass writes waits for the whole pass to complete and its stores to
+// be visible (grid_dep_wait).  Without the launch attribute the wait returns
+// at once and the trigger does nothing.
+__device__ __forceinline__ void grid_dep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void grid_dep_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
@@ -204,8 +212,12 @@ __global__ void wait_selftest_kernel(int* status, int limit) {
 // band pass to finish.
 __device__ __forceinline__ bool row_stored(const StepParams& P, int j) { return j < P.nz; }
 
-// Band scratch: output field f (0, 1[, 2] of the half step) of band row
-// jb = j - (nz-nbc-1), as planes of nbc rows with the grid's row pitch.
+// Band scratch: plane f of band row jb = j - (nz-nbc-1), planes of nbc rows
+// with the grid's row pitch.  txx, tzz, txz use planes 0-2 and vx, vz planes
+// kBandVelPlane + 0, 1, so a band pass never shares a plane with the tiles of
+// the next half step, which may run beside it.
+constexpr int kBandPlanes = 5;
+constexpr int kBandVelPlane = 3;
 __device__ __forceinline__ float* band_pre_at(const StepParams& P, const TiledArgs& T, int f, int jb, int i) {
     return T.band_pre + ((size_t)f * P.nbc + jb) * P.pitch + i;
 }
@@ -332,8 +344,8 @@ __device__ void edge_tile(const StepParams& P, const TiledArgs& T, int x0, int z
                 vx = HabcPoint<SmemPre>{P, SmemPre{spre, xa, za, G::RW, G::RH, 0}, P.in[VX], P.w_tab[0]}.final_value(i, j);
                 vz = HabcPoint<SmemPre>{P, SmemPre{spre, xa, za, G::RW, G::RH, 1}, P.in[VZ], P.w_tab[1]}.final_value(i, j);
             }
-            *store_at(P, T, P.out[VX], 0, i, j) = vx;
-            *store_at(P, T, P.out[VZ], 1, i, j) = vz;
+            *store_at(P, T, P.out[VX], kBandVelPlane, i, j) = vx;
+            *store_at(P, T, P.out[VZ], kBandVelPlane + 1, i, j) = vz;
         } else {
             float v[3];
 #pragma unroll
@@ -520,8 +532,8 @@ __device__ __forceinline__ void fast_vel(const StepParams& P, const TiledArgs& T
 #pragma unroll
         for (int rr = 0; rr < 2; ++rr)
             if (row_stored(P, zt + rr)) {
-                stg4(store_at(P, T, P.out[VX], 0, x, zt + rr), ox[rr]);
-                stg4(store_at(P, T, P.out[VZ], 1, x, zt + rr), oz[rr]);
+                stg4(store_at(P, T, P.out[VX], kBandVelPlane, x, zt + rr), ox[rr]);
+                stg4(store_at(P, T, P.out[VZ], kBandVelPlane + 1, x, zt + rr), oz[rr]);
             }
     }
 }
@@ -683,6 +695,13 @@ __device__ __forceinline__ TileKind classify(const StepParams& P, const TiledArg
     return k;
 }
 
+// A tile whose input rows (halo and edge margin included, one row to spare)
+// reach the bottom band rows nz-nbc-1 .. nz-2, which the band pass of the
+// previous half step writes.  Only these tiles wait for that pass.
+__device__ __forceinline__ bool reads_band_rows(const StepParams& P, int z0) {
+    return z0 + kTZ + kEdgeZ + P.M >= P.nz - P.nbc - 1;
+}
+
 // ---------------------------------------------------------------- receivers
 // rec_k: 1-based step recorded from P.in (P.rec_k on the single-shot path).
 __device__ inline void record_block(const StepParams& P, int rblock, int rec_k) {
@@ -704,10 +723,12 @@ __global__ void __launch_bounds__(kThreads, kTileBlocks<M>) velocity_kernel(cons
     const int bid = blockIdx.x;
     if (bid < T.n_tile_blocks) {
         const TileKind k = classify(P, T, bid);
+        if (reads_band_rows(P, k.z0)) grid_dep_wait();
         if (k.generic) edge_tile<M, true>(P, T, k.x0, k.z0, k.x_end, smem, P.src_w);
         else fast_vel<M>(P, T, refs_of(maps), k.x0, k.z0, k.x_end, k.band, k.rim, smem, P.src_w);
         return;
     }
+    grid_dep_wait();  // receivers may sit in the band rows
     record_block(P, bid - T.n_tile_blocks, P.rec_k);
 }
 
@@ -718,6 +739,7 @@ __global__ void __launch_bounds__(kThreads, kTileBlocks<M>) stress_kernel(const 
     const int bid = blockIdx.x;
     if (bid < T.n_tile_blocks) {
         const TileKind k = classify(P, T, bid);
+        if (reads_band_rows(P, k.z0)) grid_dep_wait();
         if (k.generic) edge_tile<M, false>(P, T, k.x0, k.z0, k.x_end, smem, P.src_w);
         else fast_str<M>(P, T, refs_of(maps), k.x0, k.z0, k.x_end, k.band, k.rim, smem, P.src_w);
     }
@@ -767,6 +789,7 @@ __device__ void band_march(const StepParams& P, const TiledArgs& T, int item, fl
     const int i = strip * kStripW - 2 + lane;
     const bool col_ok = i >= 0 && i < nx;
     const int q = VEL ? VX + f : TXX + f;
+    const int plane = VEL ? kBandVelPlane + f : f;
     const float* oin = in_field(P, q);
     float* oout = q == VX ? P.out[VX] : q == VZ ? P.out[VZ] : q == TXX ? P.out[TXX] : q == TZZ ? P.out[TZZ] : P.out[TXZ];
     // the lane's rule
@@ -783,7 +806,7 @@ __device__ void band_march(const StepParams& P, const TiledArgs& T, int item, fl
         for (int r = 0; r < kMarchRows; ++r) {
             const int jb = c * kMarchRows + r;
             const bool ok = col_ok && jb < b;
-            cp_async4(buf + r * 32 + lane, ok ? band_pre_at(P, T, f, jb, i) : T.band_pre, ok);
+            cp_async4(buf + r * 32 + lane, ok ? band_pre_at(P, T, plane, jb, i) : T.band_pre, ok);
             cp_async4(buf + (kMarchRows + r) * 32 + lane, ok ? oin + cell(P, i, j0 + jb) : oin, ok);
         }
         cp_async_commit();
@@ -829,11 +852,14 @@ __device__ void band_march(const StepParams& P, const TiledArgs& T, int item, fl
 }
 
 // The band pass of one half step: one warp per (strip, field) (P, T as for
-// the half step's tile launch, which must have completed).
+// the half step's tile launch, which must have completed).  The next tile
+// launch may start beside it: it writes neither the fields nor the scratch
+// planes read here, and its tiles that read the band rows wait.
 template <bool VEL>
 __global__ void __launch_bounds__(32) band_kernel(const __grid_constant__ StepParams P, const __grid_constant__ TiledArgs T) {
     __shared__ __align__(16) float stage[kMarchStage];
     __shared__ float stab[kMaxBandTab];
+    grid_dep_trigger();
     band_march<VEL>(P, T, blockIdx.x, stage, stab);
 }
 

@@ -253,7 +253,7 @@ int fomo_b200_selftest_wait(int32_t polls, int32_t* status);
  * every GPU loading the library holds until the process exits; grids whose
  * scratch does not fit are rejected with FOMO_EINVAL and a message giving
  * the bytes needed.  The scratch is 10 fields (+2 buoyancy arrays when
- * dtx == dtz, +4 otherwise) of pitch*nz floats, 3*nbc rows of pitch floats
+ * dtx == dtz, +4 otherwise) of pitch*nz floats, 5*nbc rows of pitch floats
  * for the bottom band, plus a few KB, so for example a 1000 x 1000 padded
  * grid with dtx == dtz and nbc = 50 fits.
  *

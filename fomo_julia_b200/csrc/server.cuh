@@ -10,8 +10,9 @@
 //           shot, starting it at the next batch step;
 //   run     K batch steps: per FD order (and up to 16 media), the step
 //           records, a velocity tile launch and its band pass, a stress tile
-//           launch and its band pass, each over every shot in flight
-//           (step_batch.cuh), then the step-counter advance;
+//           launch and its band pass, per launch set of up to 12 shots
+//           (step_batch.cuh); each tile launch may start beside the band
+//           pass before it (programmatic dependent launch);
 //           K steps are one CUDA graph replay once captured;
 //   retire  shots whose nt steps are done: record the last step's receivers,
 //           copy the gather to pinned memory, free the shot's memory (stream
@@ -119,6 +120,7 @@ struct Request {
 // steps), otherwise one graph of K steps.
 constexpr int kTuneK[3] = {1, 8, 32};
 constexpr int kPlainChunk = 32;
+constexpr int kMaxInFlight = 4096;  // shots in flight per server (launch sets <= shots)
 
 struct TuneKey {
     int nx, nz, M, shots_log2;
@@ -214,20 +216,22 @@ struct LaunchSet {
     size_t smem_v = 0, smem_s = 0;
 };
 
+// A set's tile launch of one half step (after_band: a dependent launch
+// beside the band pass just before it, see launch_tiles).
 template <int M>
-void launch_batch_M(bool vel, const LaunchSet& S, cudaStream_t st) {
-    if (vel) fomo::batch_velocity_kernel<M><<<S.grid_v, fomo::kThreads, S.smem_v, st>>>(*S.lv);
-    else fomo::batch_stress_kernel<M><<<S.grid_s, fomo::kThreads, S.smem_s, st>>>(*S.ls);
+void launch_batch_M(bool vel, const LaunchSet& S, cudaStream_t st, bool after_band) {
+    if (vel) launch_tiles(fomo::batch_velocity_kernel<M>, S.grid_v, S.smem_v, st, after_band, *S.lv);
+    else launch_tiles(fomo::batch_stress_kernel<M>, S.grid_s, S.smem_s, st, after_band, *S.ls);
 }
 
-void launch_batch(bool vel, const LaunchSet& S, cudaStream_t st) {
+void launch_batch(bool vel, const LaunchSet& S, cudaStream_t st, bool after_band) {
     switch (S.M) {
-        case 1: launch_batch_M<1>(vel, S, st); break;
-        case 2: launch_batch_M<2>(vel, S, st); break;
-        case 3: launch_batch_M<3>(vel, S, st); break;
-        case 4: launch_batch_M<4>(vel, S, st); break;
-        case 5: launch_batch_M<5>(vel, S, st); break;
-        case 6: launch_batch_M<6>(vel, S, st); break;
+        case 1: launch_batch_M<1>(vel, S, st, after_band); break;
+        case 2: launch_batch_M<2>(vel, S, st, after_band); break;
+        case 3: launch_batch_M<3>(vel, S, st, after_band); break;
+        case 4: launch_batch_M<4>(vel, S, st, after_band); break;
+        case 5: launch_batch_M<5>(vel, S, st, after_band); break;
+        case 6: launch_batch_M<6>(vel, S, st, after_band); break;
     }
 }
 
@@ -248,11 +252,9 @@ class Server {
         CUDA_TRY(cudaMemPoolCreate(&pool_, &props));
         uint64_t keep = UINT64_MAX;
         CUDA_TRY(cudaMemPoolSetAttribute(pool_, cudaMemPoolAttrReleaseThreshold, &keep));
-        CUDA_TRY(cudaMalloc(&d_ctl_, 256));
-        d_step_ = reinterpret_cast<int*>(d_ctl_);
+        CUDA_TRY(cudaMalloc(&d_ctl_, 256 + 2 * sizeof(int) * kMaxInFlight));
         d_status_ = reinterpret_cast<int*>(d_ctl_ + 128);
-        const int one = 1;
-        CUDA_TRY(cudaMemcpy(d_step_, &one, sizeof(int), cudaMemcpyHostToDevice));
+        d_counters_ = reinterpret_cast<int*>(d_ctl_ + 256);
         CUDA_TRY(cudaMemset(d_status_, 0, sizeof(int)));
         if (cfg_.hbm_budget_bytes == 0) {
             size_t fr = 0, tot = 0;
@@ -399,7 +401,7 @@ class Server {
     cudaStream_t st_ = nullptr;
     cudaMemPool_t pool_ = nullptr;
     unsigned char* d_ctl_ = nullptr;
-    int* d_step_ = nullptr;
+    int* d_counters_ = nullptr;   // per launch set: velocity and stress batch step
     int* d_status_ = nullptr;
     std::thread worker_;
 
@@ -735,18 +737,27 @@ class Server {
                 for (int q = 0; q < 4; ++q) S.lv->b[t][q] = r.res->bmap[q];
                 for (int q = 0; q < 3; ++q) S.ls->mod[t][q] = r.res->mod[q];
             }
-            H.step = d_step_;
+            int* cnt = d_counters_ + 2 * sets_.size();
+            H.step = cnt;
+            H.advance = cnt + 1;
             H.n_shots = (int)(j - i);
             H.n_groups = n_groups;
             H.total_band = band;
             H.total_tile = tile;
             S.ls->H = H;
+            S.ls->H.step = cnt + 1;
+            S.ls->H.advance = cnt;
             S.grid_v = tile + rec;
             S.grid_s = tile;
             S.grid_b = band;
             if (int rc = set_batch_smem(S.M, S.smem_v, S.smem_s)) return rc;
             sets_.push_back(S);
             i = j;
+        }
+        if (!sets_.empty()) {  // counters of the new sets continue at the next batch step (stream ordered)
+            const int n = (int)sets_.size();
+            fomo::batch_counters_kernel<<<(n + 255) / 256, 256, 0, st_>>>(d_counters_, n, (int)(k_host_ + 1));
+            CUDA_TRY(cudaGetLastError());
         }
         dirty_ = false;
         return FOMO_OK;
@@ -766,16 +777,20 @@ class Server {
     }
 
     // ------------------------------------------------------------ stepping
-    int launches_per_step() const { return 4 * (int)sets_.size() + 1; }
+    int launches_per_step() const { return 4 * (int)sets_.size(); }
 
-    void enqueue_step() {
-        for (const LaunchSet& S : sets_) launch_batch(true, S, st_);
-        for (const LaunchSet& S : sets_)
+    // One batch step, set after set.  `after_band`: the last launch on the
+    // stream is the previous step's last stress band pass, so the first
+    // velocity launch may start beside it (every later tile launch follows
+    // a band pass).
+    void enqueue_step(bool after_band) {
+        for (size_t i = 0; i < sets_.size(); ++i) {
+            const LaunchSet& S = sets_[i];
+            launch_batch(true, S, st_, after_band || i > 0);
             fomo::batch_band_kernel<true, fomo::BatchVelLaunch><<<S.grid_b, 32, 0, st_>>>(*S.lv);
-        for (const LaunchSet& S : sets_) launch_batch(false, S, st_);
-        for (const LaunchSet& S : sets_)
+            launch_batch(false, S, st_, true);
             fomo::batch_band_kernel<false, fomo::BatchStrLaunch><<<S.grid_b, 32, 0, st_>>>(*S.ls);
-        fomo::batch_advance_kernel<<<1, 1, 0, st_>>>(d_step_);
+        }
     }
 
     int graph_for(int K, cudaGraphExec_t* out) {
@@ -786,7 +801,7 @@ class Server {
         }
         cudaGraph_t g = nullptr;
         CUDA_TRY(cudaStreamBeginCapture(st_, cudaStreamCaptureModeThreadLocal));
-        for (int k = 0; k < K; ++k) enqueue_step();
+        for (int k = 0; k < K; ++k) enqueue_step(k > 0);
         cudaError_t e = cudaStreamEndCapture(st_, &g);
         if (e != cudaSuccess) return fail(FOMO_ECUDA, "graph capture failed: %s", cudaGetErrorString(e));
         cudaGraphExec_t x = nullptr;
@@ -893,7 +908,7 @@ class Server {
             nvtxRangePop();
             CUDA_TRY(e);
         } else {
-            for (int k = 0; k < n; ++k) enqueue_step();
+            for (int k = 0; k < n; ++k) enqueue_step(k > 0);
             nvtxRangePop();
             CUDA_TRY(cudaGetLastError());
         }
@@ -1037,6 +1052,7 @@ class Server {
                 while (!queue_.empty()) {
                     Request& r = *queue_.front();
                     if (cfg_.max_shots > 0 && (int)(active_.size() + admitted.size()) >= cfg_.max_shots) break;
+                    if (active_.size() + admitted.size() >= (size_t)kMaxInFlight) break;
                     auto key = res_key(r);
                     const bool have = resident_.count(key) != 0 ||
                                       std::find(new_res.begin(), new_res.end(), key) != new_res.end();

@@ -5,10 +5,22 @@
 // constant cache): for every shot, its StepParams for both wavefield copies
 // it may read (in/out pointers differ by the parity of the local step), its
 // TiledArgs, its start step and wavelet, and its TMA descriptors.  The batch
-// step comes from a device counter, so every launch of a batch has the same
+// step comes from device counters, so every launch of a batch has the same
 // arguments and a run of K time steps (tile and band launches of velocity
-// and stress, then the counter advance) can be captured once into a CUDA
-// graph and replayed.
+// and stress) can be captured once into a CUDA graph and replayed.
+//
+// A launch set (up to kShotsPerLaunch shots) runs velocity tiles, velocity
+// band pass, stress tiles, stress band pass, then the next set; every tile
+// launch may start beside the band pass just before it (programmatic
+// dependent launch), so each set has two counters: its velocity launches
+// (tiles and band) read the velocity counter, its stress launches the
+// stress counter.  Block 0 of the velocity tile launch waits for the launch
+// before it and advances the stress counter to the step; block 0 of the
+// stress tile launch waits for the velocity band pass and advances the
+// velocity counter to the next step.  Nothing reads a counter while it is
+// advanced: a tile launch overlaps only the band pass just before it, which
+// block 0 has waited for, and the launches that read the counter next start
+// after the advancing launch has completed.
 //
 // Shots are grouped by medium (same nx, nz, hence the same block counts).  A
 // tile launch holds, for every shot s whose local step ks = k - start_s + 1
@@ -44,7 +56,8 @@ struct GroupDev {
 };
 
 struct BatchHead {
-    const int* step;                  // batch step (1-based), advanced once per step
+    const int* step;                  // batch step (1-based) of the launch's half step
+    int* advance;                     // the other half step's counter of the set (block 0 advances it)
     int n_shots, n_groups;
     int total_band, total_tile;
     int rec_off[kShotsPerLaunch + 1]; // first receiver block of each shot
@@ -131,15 +144,36 @@ __device__ __forceinline__ float wavelet_at(const BatchShot& S, int ks) {
     return (ks >= 1 && ks <= S.n_wavelet) ? __ldg(S.wavelet + ks - 1) : 0.f;
 }
 
+// Block 0 of a tile launch: waits for the launches before it (always, so
+// the launch cannot complete before them) and advances the other counter.
+__device__ __forceinline__ void block0_advance(const BatchHead& H) {
+    if (blockIdx.x != 0) return;
+    grid_dep_wait();
+    if (threadIdx.x == 0 && H.advance) *H.advance += 1;
+}
+
+// Sets the counters of n launch sets when the host rebuilds its tables:
+// velocity counter of set i (counters[2i]) to `step`, stress counter
+// (counters[2i+1]) to step - 1.
+__global__ void batch_counters_kernel(int* counters, int n, int step) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) {
+        counters[2 * i] = step;
+        counters[2 * i + 1] = step - 1;
+    }
+}
+
 template <int M>
 __global__ void __launch_bounds__(kThreads, kTileBlocks<M>) batch_velocity_kernel(const __grid_constant__ BatchVelLaunch L) {
     extern __shared__ __align__(128) float smem[];
+    block0_advance(L.H);
     const BatchItem it = decode(L.H, blockIdx.x, true, false);
     if (it.role < 0) return;
     const BatchShot& S = L.shot[it.shot];
     const int ks = local_step(L.H, S);
     const int a = (ks - 1) & 1;
     if (it.role == 2) {
+        grid_dep_wait();  // receivers may sit in the band rows
         if (ks >= 2 && ks <= S.nt + 1) record_block(S.P[a], it.local, ks - 1);  // state after step ks-1: copy a
         return;
     }
@@ -147,6 +181,7 @@ __global__ void __launch_bounds__(kThreads, kTileBlocks<M>) batch_velocity_kerne
     const float src_w = wavelet_at(S, ks);
     const StepParams& P = S.P[a];
     const TileKind k = classify(P, S.T, it.local);
+    if (reads_band_rows(P, k.z0)) grid_dep_wait();
     if (k.generic) {
         edge_tile<M, true>(P, S.T, k.x0, k.z0, k.x_end, smem, src_w);
     } else {
@@ -160,6 +195,7 @@ __global__ void __launch_bounds__(kThreads, kTileBlocks<M>) batch_velocity_kerne
 template <int M>
 __global__ void __launch_bounds__(kThreads, kTileBlocks<M>) batch_stress_kernel(const __grid_constant__ BatchStrLaunch L) {
     extern __shared__ __align__(128) float smem[];
+    block0_advance(L.H);
     const BatchItem it = decode(L.H, blockIdx.x, false, false);
     if (it.role < 0) return;
     const BatchShot& S = L.shot[it.shot];
@@ -169,6 +205,7 @@ __global__ void __launch_bounds__(kThreads, kTileBlocks<M>) batch_stress_kernel(
     const float src_w = wavelet_at(S, ks);
     const StepParams& P = S.P[a];
     const TileKind k = classify(P, S.T, it.local);
+    if (reads_band_rows(P, k.z0)) grid_dep_wait();
     if (k.generic) {
         edge_tile<M, false>(P, S.T, k.x0, k.z0, k.x_end, smem, src_w);
     } else {
@@ -186,15 +223,12 @@ template <bool VEL, class LaunchT>
 __global__ void __launch_bounds__(32) batch_band_kernel(const __grid_constant__ LaunchT L) {
     __shared__ __align__(16) float stage[kMarchStage];
     __shared__ float stab[kMaxBandTab];
+    grid_dep_trigger();
     const BatchItem it = decode(L.H, blockIdx.x, VEL, true);
     const BatchShot& S = L.shot[it.shot];
     const int ks = local_step(L.H, S);
     if (ks < 1 || ks > S.nt) return;
     band_march<VEL>(S.P[(ks - 1) & 1], S.T, it.local, stage, stab);
 }
-
-// Advances the batch step counter; launched once per step after the last
-// launch of the step.
-__global__ void batch_advance_kernel(int* step) { *step += 1; }
 
 }  // namespace fomo

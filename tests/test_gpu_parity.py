@@ -5,6 +5,8 @@ with IEEE rounding, so gathers and final wavefields are expected to be
 bit-identical to the oracle; the acceptance bar stated by the spec
 (relative L2 <= 1e-5 per trace) is asserted as well.
 """
+import dataclasses
+
 import numpy as np
 import pytest
 
@@ -56,6 +58,12 @@ def assert_same(g_gpu, g_orc, f_gpu, f_orc, exact=True):
             assert np.array_equal(f_gpu[f], f_orc[f]), f"field {f} not bit-identical"
 
 
+def _anisotropic_grid_case():
+    # dz != dx: four buoyancy arrays (dtx/rho and dtz/rho differ)
+    c = layered(236, 92, seed=19, nbc=11, fd_order=8, nt=90, n_rec=19)
+    return dataclasses.replace(c, dz=13.0, name=c.name + "dz13")
+
+
 def _band_source_case():
     # source inside the left HABC band and the bottom band (bottom-left corner)
     c = layered(38, 30, seed=11, nbc=6, fd_order=8, nt=140)
@@ -90,6 +98,11 @@ CASES = [
     layered(205, 75, seed=14, nbc=12, fd_order=12, nt=90, free_surface=False, rec_type="p"),
     layered(150, 70, seed=15, nbc=60, fd_order=4, nt=80, rec_type="vx"),   # band wider than a fast tile allows
     layered(190, 96, seed=16, nbc=20, fd_order=6, nt=90, water_rows=6, n_rec=23),
+    # wide grids: interior tiles without a free surface (source deep inside), order 2, dz != dx
+    layered(260, 110, seed=17, nbc=12, fd_order=8, nt=90, free_surface=False, rec_type="p", n_rec=29,
+            src=(10.0 * 130 + 5.0, 10.0 * 50)),
+    layered(250, 84, seed=18, nbc=9, fd_order=2, nt=80, rec_type="vx"),
+    _anisotropic_grid_case(),
 ]
 
 

@@ -56,6 +56,13 @@ struct Buffer : Object {
     }
 };
 
+// Device memory of media, wavefields and shots comes from a per-device
+// stream-ordered pool (on the library stream) that keeps what is freed, so
+// creating and destroying them again and again costs no driver allocation
+// and no device-wide synchronisation (cudaFree has both).
+cudaError_t pool_alloc(void** p, size_t bytes);
+void pool_free(void* p);
+
 // Row pitch in floats: rows start on 128-byte boundaries.
 inline int pitch_of(int nx) { return (nx + 31) / 32 * 32; }
 
@@ -74,8 +81,8 @@ struct Medium : Object {
     std::atomic<int> users{0}; // shot-server requests holding this medium
     const float* arr(int q) const { return base + (size_t)q * pitch * nz; }
     ~Medium() override {
-        if (base) cudaFree(base);
-        if (buoy) cudaFree(buoy);
+        pool_free(base);
+        pool_free(buoy);
     }
 };
 
@@ -90,8 +97,8 @@ struct Wavefield : Object {
     size_t snap_bytes = 0;
     float* field(int copy, int q) const { return base + ((size_t)copy * 5 + q) * pitch * nz; }
     ~Wavefield() override {
-        if (base) cudaFree(base);
-        if (snap) cudaFree(snap);
+        pool_free(base);
+        pool_free(snap);
     }
 };
 
@@ -112,10 +119,10 @@ struct Shot : Object {
     double device_ms = 0;
     int64_t launches = 0, h2d = 0, d2h = 0;
     ~Shot() override {
-        if (d_tabs) cudaFree(d_tabs);
-        if (d_band) cudaFree(d_band);
-        if (d_rec) cudaFree(d_rec);
-        if (d_gather) cudaFree(d_gather);
+        pool_free(d_tabs);
+        pool_free(d_band);
+        pool_free(d_rec);
+        pool_free(d_gather);
     }
 };
 
@@ -126,6 +133,7 @@ struct Context {
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     int* d_status = nullptr;   // device error word of the kernels
+    cudaMemPool_t pool = nullptr;
     uint64_t next = 1;
     std::unordered_map<uint64_t, std::unique_ptr<Object>> objs;
 };
@@ -133,6 +141,26 @@ struct Context {
 Context& ctx() {
     static Context c;
     return c;
+}
+
+cudaError_t pool_alloc(void** p, size_t bytes) {
+    auto& C = ctx();
+    cudaError_t e = cudaMallocFromPoolAsync(p, bytes, C.pool, C.stream);
+    if (e == cudaErrorMemoryAllocation) {  // give the pool's cached memory back to the device, then retry once
+        (void)cudaGetLastError();
+        cudaStreamSynchronize(C.stream);
+        cudaMemPoolTrimTo(C.pool, 0);
+        e = cudaMallocFromPoolAsync(p, bytes, C.pool, C.stream);
+    }
+    if (e != cudaSuccess) {
+        (void)cudaGetLastError();  // not a sticky error: the caller reports it
+        *p = nullptr;
+    }
+    return e;
+}
+
+void pool_free(void* p) {
+    if (p) cudaFreeAsync(p, ctx().stream);
 }
 
 template <class T>
@@ -228,7 +256,7 @@ int ensure_buoyancy(Medium& m, float dtx, float dtz) {
     if (m.buoy && m.buoy_dtx == dtx && m.buoy_dtz == dtz) return FOMO_OK;
     const size_t plane = (size_t)m.pitch * m.nz;
     if (!m.buoy) {
-        cudaError_t e = cudaMalloc(&m.buoy, 4 * plane * sizeof(float));
+        cudaError_t e = pool_alloc((void**)&m.buoy, 4 * plane * sizeof(float));
         if (e != cudaSuccess) return fail(FOMO_ENOMEM, "buoyancy allocation failed: %s", cudaGetErrorString(e));
     }
     float* b0 = m.buoy;
@@ -507,6 +535,15 @@ int fomo_b200_init(int device) {
     CUDA_TRY(cudaEventCreate(&C.ev1));
     CUDA_TRY(cudaMalloc(&C.d_status, sizeof(int)));
     CUDA_TRY(cudaMemset(C.d_status, 0, sizeof(int)));
+    cudaMemPoolProps props;
+    std::memset(&props, 0, sizeof(props));
+    props.allocType = cudaMemAllocationTypePinned;
+    props.handleTypes = cudaMemHandleTypeNone;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = device;
+    CUDA_TRY(cudaMemPoolCreate(&C.pool, &props));
+    uint64_t keep = UINT64_MAX;
+    CUDA_TRY(cudaMemPoolSetAttribute(C.pool, cudaMemPoolAttrReleaseThreshold, &keep));
     C.device = device;
     C.inited = true;
     return FOMO_OK;
@@ -519,6 +556,9 @@ int fomo_b200_shutdown(void) {
     if (!C.inited) return FOMO_OK;
     cudaStreamSynchronize(C.stream);
     C.objs.clear();
+    cudaStreamSynchronize(C.stream);
+    cudaMemPoolDestroy(C.pool);
+    C.pool = nullptr;
     cudaEventDestroy(C.ev0);
     cudaEventDestroy(C.ev1);
     cudaFree(C.d_status);
@@ -626,7 +666,7 @@ int fomo_b200_medium_create(int32_t nx, int32_t nz, int32_t M, int32_t pad, int3
     m->dx = dx;
     m->dz = dz;
     const size_t plane = (size_t)m->pitch * nz;
-    cudaError_t e = cudaMalloc(&m->base, 5 * plane * sizeof(float));
+    cudaError_t e = pool_alloc((void**)&m->base, 5 * plane * sizeof(float));
     if (e != cudaSuccess) return fail(FOMO_ENOMEM, "medium allocation failed: %s", cudaGetErrorString(e));
     const float* src[5] = {rho_vx, rho_vz, lam, mu_txx, mu_txz};
     for (int q = 0; q < 5; ++q)
@@ -660,12 +700,9 @@ int fomo_b200_medium_create_from_model(int32_t nx_in, int32_t nz_in, const float
     const size_t plane = (size_t)m->pitch * nz;
     const size_t model = (size_t)nx_in * nz_in;
     float* d_model = nullptr;
-    cudaError_t e = cudaMalloc(&m->base, 5 * plane * sizeof(float));
-    if (e == cudaSuccess) e = cudaMalloc(&d_model, 3 * model * sizeof(float));
-    if (e != cudaSuccess) {
-        if (d_model) cudaFree(d_model);
-        return fail(FOMO_ENOMEM, "medium allocation failed: %s", cudaGetErrorString(e));
-    }
+    cudaError_t e = pool_alloc((void**)&m->base, 5 * plane * sizeof(float));
+    if (e == cudaSuccess) e = pool_alloc((void**)&d_model, 3 * model * sizeof(float));
+    if (e != cudaSuccess) return fail(FOMO_ENOMEM, "medium allocation failed: %s", cudaGetErrorString(e));
     cudaStream_t st = ctx().stream;
     const float* src[3] = {vp, vs, rho};
     int rc = FOMO_OK;
@@ -678,8 +715,8 @@ int fomo_b200_medium_create_from_model(int32_t nx_in, int32_t nz_in, const float
                                                           m->base + 2 * plane, m->base + 3 * plane, m->base + 4 * plane);
         if (cudaGetLastError() != cudaSuccess) rc = fail(FOMO_ECUDA, "medium set-up kernel launch failed");
     }
+    pool_free(d_model);
     cudaStreamSynchronize(st);
-    cudaFree(d_model);
     if (rc) return rc;
     *medium = put(std::move(m));
     return FOMO_OK;
@@ -719,7 +756,7 @@ int fomo_b200_wavefield_create(int32_t nx, int32_t nz, uint64_t* wavefield) {
     w->nz = nz;
     w->pitch = pitch_of(nx);
     const size_t bytes = 10 * (size_t)w->pitch * nz * sizeof(float);
-    cudaError_t e = cudaMalloc(&w->base, bytes);
+    cudaError_t e = pool_alloc((void**)&w->base, bytes);
     if (e != cudaSuccess) return fail(FOMO_ENOMEM, "wavefield allocation of %zu bytes failed: %s", bytes, cudaGetErrorString(e));
     CUDA_TRY(cudaMemsetAsync(w->base, 0, bytes, ctx().stream));
     CUDA_TRY(cudaStreamSynchronize(ctx().stream));
@@ -785,10 +822,10 @@ int fomo_b200_wavefield_snapshot(uint64_t wavefield, int32_t kind, int32_t downs
     const int nx_d = (w->nx + downsample - 1) / downsample, nz_d = (w->nz + downsample - 1) / downsample;
     const size_t bytes = (size_t)nx_d * nz_d * sizeof(float);
     if (bytes > w->snap_bytes) {
-        if (w->snap) cudaFree(w->snap);
+        pool_free(w->snap);
         w->snap = nullptr;
         w->snap_bytes = 0;
-        cudaError_t e = cudaMalloc(&w->snap, bytes);
+        cudaError_t e = pool_alloc((void**)&w->snap, bytes);
         if (e != cudaSuccess) return fail(FOMO_ENOMEM, "snapshot buffer of %zu bytes failed", bytes);
         w->snap_bytes = bytes;
     }
@@ -855,11 +892,11 @@ int fomo_b200_shot_begin(uint64_t medium, uint64_t wavefield, const FomoHabc* ha
     s->n_rec = shot->n_rec;
     s->rec_kind = shot->rec_kind;
     const size_t tab_n = (size_t)nbc + 2;
-    cudaError_t e = cudaMalloc(&s->d_tabs, 3 * tab_n * sizeof(float));
-    if (e == cudaSuccess) e = cudaMalloc(&s->d_band, fomo::kBandPlanes * (size_t)nbc * m->pitch * sizeof(float));
-    if (e == cudaSuccess && s->n_rec) e = cudaMalloc(&s->d_rec, s->n_rec * sizeof(int));
+    cudaError_t e = pool_alloc((void**)&s->d_tabs, 3 * tab_n * sizeof(float));
+    if (e == cudaSuccess) e = pool_alloc((void**)&s->d_band, fomo::kBandPlanes * (size_t)nbc * m->pitch * sizeof(float));
+    if (e == cudaSuccess && s->n_rec) e = pool_alloc((void**)&s->d_rec, s->n_rec * sizeof(int));
     if (e == cudaSuccess && s->n_rec && s->nt)
-        e = cudaMalloc(&s->d_gather, (size_t)s->nt * s->n_rec * sizeof(float));
+        e = pool_alloc((void**)&s->d_gather, (size_t)s->nt * s->n_rec * sizeof(float));
     if (e != cudaSuccess) return fail(FOMO_ENOMEM, "shot allocation failed: %s", cudaGetErrorString(e));
     cudaStream_t st = ctx().stream;
     CUDA_TRY(cudaMemcpyAsync(s->d_tabs, habc->w_vx, tab_n * 4, cudaMemcpyHostToDevice, st));

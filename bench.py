@@ -196,6 +196,14 @@ def reference_arm(args, rank, world):
 
 
 # ---------------------------------------------------------------- batched and served shots
+def hbm_peak():
+    """HBM bandwidth denominator: MEASURED_PEAKS.json hbm_gbs, else the fallback figure."""
+    try:
+        return float(json.load(open(os.path.join(REPO, "MEASURED_PEAKS.json")))["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
 def batched_section(args):
     """64 shots on one 2000 x 800 medium: sequential plain shots
     (fomo_b200_run_shot, one after another) against one fomo_b200_run_batch
@@ -244,9 +252,21 @@ def batched_section(args):
         "batched_shots_per_hour": n * 3600.0 / t_batch,
         "speedup_vs_plain": (n * 3600.0 / t_batch) / (3600.0 / t_plain),
         "batched_gcell_steps_s": n * cells * nt / t_batch / 1e9,
+        "roofline": batched_roofline(n * cells * nt, res[0].stats["device_ms"] / 1e3),
         "batched_launches": res[0].stats["kernel_launches"],
         "gathers_identical_to_plain": bool(same),
     }
+
+
+def batched_roofline(shot_cell_steps, device_s, shots_per_pass=12):
+    """Batched throughput against the one-pass byte minimum with S shots sharing a
+    medium pass: 40 B per shot-cell-step of fields (read and write the five) plus
+    20/S B of medium (read once per launch set of up to 12 shots)."""
+    peak, src = hbm_peak()
+    b = 40.0 + 20.0 / shots_per_pass
+    gbs = shot_cell_steps * b / device_s / 1e9
+    return {"bytes_per_shot_cell_step": b, "basis": f"one pass per step, medium read once per {shots_per_pass} shots",
+            "achieved_gbs": gbs, "peak": peak, "peak_source": src, "frac": gbs / peak}
 
 
 def uneven_section(args):
@@ -538,12 +558,7 @@ def b200_arm(args, rank, world, local):
             avg = k.total_ms / k.launches
             kernels.append({"name": k.name.decode(), "launches": k.launches, "avg_ms": avg,
                             "bytes_per_launch": k.bytes_per_launch, "gbs": k.bytes_per_launch / (avg / 1e3) / 1e9})
-    peaks = {}
-    try:
-        peaks = json.load(open(os.path.join(REPO, "MEASURED_PEAKS.json")))
-        peak, peak_src = float(peaks["hbm_gbs"]), "measured"
-    except Exception:
-        peak, peak_src = 6650.0, "fallback"
+    peak, peak_src = hbm_peak()
     dom = max(kernels, key=lambda k: k["avg_ms"] * k["launches"]) if kernels else None
     # one time step of the timed shots (band passes overlap the tile launches there, so this
     # is below the sum of the separately timed launches)
@@ -564,6 +579,9 @@ def b200_arm(args, rank, world, local):
                     "step_achieved": 60.0 * cells / (step_ms / 1e3) / 1e9,
                     "step_frac": (60.0 * cells / (step_ms / 1e3) / 1e9) / peak,
                     "launches_sum_ms": sum(k["avg_ms"] for k in kernels),
+                    # perimeter work: the bottom-band passes, as a share of the launches timed one by one
+                    "perimeter_frac": sum(k["avg_ms"] for k in kernels if k["name"].startswith("band"))
+                    / sum(k["avg_ms"] for k in kernels),
                     "kernels": kernels}
 
     cpu = None
@@ -598,6 +616,9 @@ def b200_arm(args, rank, world, local):
                        "shots_per_gpu_per_step": 1, "parallelism": f"shot-sharded x{world}",
                        "l2": "inputs larger than L2 (357 MB medium + 715 MB state per shot)",
                        "bytes_per_cell_step_algorithmic": 60},
+            "physical_cells": {"cells": w.nx_in * w.nz_in,
+                               "value": value * (w.nx_in * w.nz_in) / cells,
+                               "note": "the same run counted on the unpadded model cells, as the reference's README counts"},
             "loop_ms_per_shot": [round(t.device_ms, 2) for t in st_v],
             "e2e": e2e, "gpu_launches": int(launches), "clocks": clocks, "roofline": roofline,
             "cpu_baseline": cpu,

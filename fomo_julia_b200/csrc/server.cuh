@@ -129,7 +129,9 @@ struct TuneKey {
     }
 };
 struct TuneEntry {
-    double ms_per_step[3] = {-1, -1, -1};
+    // device time per cell-step of the shots in flight (ms per Gcell-step):
+    // comparable across chunks whose shots differ
+    double ms_per_work[3] = {-1, -1, -1};
     int chosen = -1;
 };
 std::mutex g_tune_mu;
@@ -391,7 +393,7 @@ class Server {
     struct Measure {   // a timed chunk of the autotuner
         TuneKey key;
         int cand;
-        int steps;
+        double work;     // Gcell-steps of the chunk: steps x cells of the shots in flight
         cudaEvent_t a, b;
     };
 
@@ -808,6 +810,9 @@ class Server {
         e = cudaGraphInstantiate(&x, g, 0);
         cudaGraphDestroy(g);
         if (e != cudaSuccess) return fail(FOMO_ECUDA, "graph instantiation failed: %s", cudaGetErrorString(e));
+        // upload now, so the first replay (maybe a timed one) does not carry it
+        e = cudaGraphUpload(x, st_);
+        if (e != cudaSuccess) return fail(FOMO_ECUDA, "graph upload failed: %s", cudaGetErrorString(e));
         graphs_[K] = x;
         *out = x;
         return FOMO_OK;
@@ -836,7 +841,7 @@ class Server {
         TuneEntry& e = g_tune[key];
         if (e.chosen >= 0) return e.chosen;
         for (int c = 0; c < 3; ++c)
-            if (e.ms_per_step[c] < 0) {
+            if (e.ms_per_work[c] < 0) {
                 bool pending = false;
                 for (auto& m : measures_)
                     if (!(m.key < key) && !(key < m.key) && m.cand == c) pending = true;
@@ -861,12 +866,12 @@ class Server {
             {
                 std::lock_guard<std::mutex> lk(g_tune_mu);
                 TuneEntry& e = g_tune[m.key];
-                e.ms_per_step[m.cand] = ms / m.steps;
+                e.ms_per_work[m.cand] = ms / m.work;
                 bool all = true;
                 int best = 0;
                 for (int c = 0; c < 3; ++c) {
-                    if (e.ms_per_step[c] < 0) all = false;
-                    else if (e.ms_per_step[best] < 0 || e.ms_per_step[c] < e.ms_per_step[best]) best = c;
+                    if (e.ms_per_work[c] < 0) all = false;
+                    else if (e.ms_per_work[best] < 0 || e.ms_per_work[c] < e.ms_per_work[best]) best = c;
                 }
                 if (all && e.chosen < 0) {
                     e.chosen = best;
@@ -895,9 +900,11 @@ class Server {
             if (int rc = graph_for(K, &x)) return rc;
         Measure ms{};
         if (measure) {
+            double cells = 0;
+            for (auto& r : active_) cells += (double)r->med->nx * r->med->nz;
             ms.key = key;
             ms.cand = cand;
-            ms.steps = n;
+            ms.work = n * cells / 1e9;
             ms.a = event(true);
             ms.b = event(true);
             CUDA_TRY(cudaEventRecord(ms.a, st_));

@@ -16,7 +16,12 @@
  *   - Grid indices passed in (source, receivers) are 1-based, as Julia
  *     passes them.
  *   - Host pointers are borrowed for the duration of the call only.  The
- *     library owns all device memory it allocates.
+ *     library owns all device memory it allocates.  Media, wavefields and
+ *     shots come from a per-device stream-ordered memory pool that keeps
+ *     freed memory for reuse (destroying them returns memory to the pool,
+ *     not to the device; fomo_b200_shutdown releases it).  When an
+ *     allocation fails, the pool gives its cached memory back to the device
+ *     and the allocation is tried once more before FOMO_ENOMEM.
  *   - Gathers are [nt x n_rec] column major: sample k (1-based) of receiver r
  *     (1-based) at (k-1) + (r-1)*nt, exactly the reference's Receivers.data.
  */

@@ -433,24 +433,28 @@ __device__ __forceinline__ void fast_vel(const StepParams& P, const TiledArgs& T
     float* p_b2 = p_b0 + kPBox;
     float* p_b1 = T.iso ? p_b0 : p_b2 + kPBox;
     float* p_b3 = T.iso ? p_b2 : p_b2 + 2 * kPBox;
+    // bar[0]: the halo boxes (the derivatives start once they land), bar[1]:
+    // the tile boxes (read by the update after the derivatives)
     uint64_t* bar = reinterpret_cast<uint64_t*>(p_b2 + (T.iso ? 1 : 3) * kPBox);
     if (threadIdx.x == 0) {
         mbar_init(bar, 1);
+        mbar_init(bar + 1, 1);
         fence_barrier_init();
     }
     __syncthreads();
     if (threadIdx.x == 0) {
-        mbar_expect_tx(bar, (3 * G::BOXW * G::BOXH + (T.iso ? 4 : 6) * kPBox) * 4);
+        mbar_expect_tx(bar, 3 * G::BOXW * G::BOXH * 4);
         tma_load_2d(s_xx, mp.xx, x0 - G::HX, z0 - M, bar);
         tma_load_2d(s_zz, mp.zz, x0 - G::HX, z0 - M, bar);
         tma_load_2d(s_xz, mp.xz, x0 - G::HX, z0 - M, bar);
-        tma_load_2d(p_vx, mp.vx, x0, z0, bar);
-        tma_load_2d(p_vz, mp.vz, x0, z0, bar);
-        tma_load_2d(p_b0, mp.b0, x0, z0, bar);
-        tma_load_2d(p_b2, mp.b2, x0, z0, bar);
+        mbar_expect_tx(bar + 1, (T.iso ? 4 : 6) * kPBox * 4);
+        tma_load_2d(p_vx, mp.vx, x0, z0, bar + 1);
+        tma_load_2d(p_vz, mp.vz, x0, z0, bar + 1);
+        tma_load_2d(p_b0, mp.b0, x0, z0, bar + 1);
+        tma_load_2d(p_b2, mp.b2, x0, z0, bar + 1);
         if (!T.iso) {
-            tma_load_2d(p_b1, mp.b1, x0, z0, bar);
-            tma_load_2d(p_b3, mp.b3, x0, z0, bar);
+            tma_load_2d(p_b1, mp.b1, x0, z0, bar + 1);
+            tma_load_2d(p_b3, mp.b3, x0, z0, bar + 1);
         }
     }
     if (!wait_tma(bar, T)) return;
@@ -486,6 +490,7 @@ __device__ __forceinline__ void fast_vel(const StepParams& P, const TiledArgs& T
         for (int k = 0; k <= 2 * M; ++k) wz[k] = lds4(s_zz + (2 * rp + 1 + k) * G::BOXW + xr + G::HX);
         zderiv<M>(P, wz, d4lo, d4hi);  // dtzz/dz: tzz[j+l] - tzz[j-l+1]
     }
+    if (!wait_tma(bar + 1, T)) return;
     float4 ox[2], oz[2];
 #pragma unroll
     for (int rr = 0; rr < 2; ++rr) {
@@ -551,22 +556,25 @@ __device__ __forceinline__ void fast_str(const StepParams& P, const TiledArgs& T
     float* p_lam = p_xz + kPBox;
     float* p_mu = p_lam + kPBox;
     float* p_mxz = p_mu + kPBox;
+    // bar[0]: the halo boxes, bar[1]: the tile boxes (as in fast_vel)
     uint64_t* bar = reinterpret_cast<uint64_t*>(p_mxz + kPBox);
     if (threadIdx.x == 0) {
         mbar_init(bar, 1);
+        mbar_init(bar + 1, 1);
         fence_barrier_init();
     }
     __syncthreads();
     if (threadIdx.x == 0) {
-        mbar_expect_tx(bar, (2 * G::BOXW * G::BOXH + 6 * kPBox) * 4);
+        mbar_expect_tx(bar, 2 * G::BOXW * G::BOXH * 4);
         tma_load_2d(s_vx, mp.vx, x0 - G::HX, z0 - M, bar);
         tma_load_2d(s_vz, mp.vz, x0 - G::HX, z0 - M, bar);
-        tma_load_2d(p_xx, mp.txx, x0, z0, bar);
-        tma_load_2d(p_zz, mp.tzz, x0, z0, bar);
-        tma_load_2d(p_xz, mp.txz, x0, z0, bar);
-        tma_load_2d(p_lam, mp.lam, x0, z0, bar);
-        tma_load_2d(p_mu, mp.mu, x0, z0, bar);
-        tma_load_2d(p_mxz, mp.mxz, x0, z0, bar);
+        mbar_expect_tx(bar + 1, 6 * kPBox * 4);
+        tma_load_2d(p_xx, mp.txx, x0, z0, bar + 1);
+        tma_load_2d(p_zz, mp.tzz, x0, z0, bar + 1);
+        tma_load_2d(p_xz, mp.txz, x0, z0, bar + 1);
+        tma_load_2d(p_lam, mp.lam, x0, z0, bar + 1);
+        tma_load_2d(p_mu, mp.mu, x0, z0, bar + 1);
+        tma_load_2d(p_mxz, mp.mxz, x0, z0, bar + 1);
     }
     if (!wait_tma(bar, T)) return;
 
@@ -593,6 +601,7 @@ __device__ __forceinline__ void fast_str(const StepParams& P, const TiledArgs& T
         for (int k = 0; k <= 2 * M; ++k) wz[k] = lds4(s_vx + (2 * rp + 1 + k) * G::BOXW + xr + G::HX);
         zderiv<M>(P, wz, dxzlo, dxzhi);  // vx[j+l] - vx[j-l+1]
     }
+    if (!wait_tma(bar + 1, T)) return;
     float4 oxx[2], ozz[2], oxz[2];
     const float2 dtx2 = make_float2(P.dtx, P.dtx), dtz2 = make_float2(P.dtz, P.dtz), two = make_float2(2.f, 2.f);
 #pragma unroll

@@ -436,13 +436,12 @@ __device__ __forceinline__ void fast_vel(const StepParams& P, const TiledArgs& T
     // bar[0]: the halo boxes (the derivatives start once they land), bar[1]:
     // the tile boxes (read by the update after the derivatives)
     uint64_t* bar = reinterpret_cast<uint64_t*>(p_b2 + (T.iso ? 1 : 3) * kPBox);
+    // thread 0 starts the copies before the block barrier that lets the
+    // other threads see the initialised mbarriers
     if (threadIdx.x == 0) {
         mbar_init(bar, 1);
         mbar_init(bar + 1, 1);
         fence_barrier_init();
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
         mbar_expect_tx(bar, 3 * G::BOXW * G::BOXH * 4);
         tma_load_2d(s_xx, mp.xx, x0 - G::HX, z0 - M, bar);
         tma_load_2d(s_zz, mp.zz, x0 - G::HX, z0 - M, bar);
@@ -457,6 +456,7 @@ __device__ __forceinline__ void fast_vel(const StepParams& P, const TiledArgs& T
             tma_load_2d(p_b3, mp.b3, x0, z0, bar + 1);
         }
     }
+    __syncthreads();
     if (!wait_tma(bar, T)) return;
     if (threadIdx.x == 0) {
         const int si = P.src_i - (x0 - G::HX), sj = P.src_j - (z0 - M);
@@ -558,13 +558,10 @@ __device__ __forceinline__ void fast_str(const StepParams& P, const TiledArgs& T
     float* p_mxz = p_mu + kPBox;
     // bar[0]: the halo boxes, bar[1]: the tile boxes (as in fast_vel)
     uint64_t* bar = reinterpret_cast<uint64_t*>(p_mxz + kPBox);
-    if (threadIdx.x == 0) {
+    if (threadIdx.x == 0) {  // copies started before the block barrier, as in fast_vel
         mbar_init(bar, 1);
         mbar_init(bar + 1, 1);
         fence_barrier_init();
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
         mbar_expect_tx(bar, 2 * G::BOXW * G::BOXH * 4);
         tma_load_2d(s_vx, mp.vx, x0 - G::HX, z0 - M, bar);
         tma_load_2d(s_vz, mp.vz, x0 - G::HX, z0 - M, bar);
@@ -576,6 +573,7 @@ __device__ __forceinline__ void fast_str(const StepParams& P, const TiledArgs& T
         tma_load_2d(p_mu, mp.mu, x0, z0, bar + 1);
         tma_load_2d(p_mxz, mp.mxz, x0, z0, bar + 1);
     }
+    __syncthreads();
     if (!wait_tma(bar, T)) return;
 
     const int cg = threadIdx.x % kCG, rp = threadIdx.x / kCG;

@@ -458,14 +458,17 @@ __device__ __forceinline__ void fast_vel(const StepParams& P, const TiledArgs& T
     }
     __syncthreads();
     if (!wait_tma(bar, T)) return;
-    if (threadIdx.x == 0) {
-        const int si = P.src_i - (x0 - G::HX), sj = P.src_j - (z0 - M);
-        if (si >= 0 && si < G::BOXW && sj >= 0 && sj < G::BOXH) {
+    // The source, added to the stresses read: only the block whose halo box
+    // holds it needs a block barrier (the condition is block-uniform; every
+    // other thread sees the boxes through its own wait on bar[0]).
+    const int si = P.src_i - (x0 - G::HX), sj = P.src_j - (z0 - M);
+    if (si >= 0 && si < G::BOXW && sj >= 0 && sj < G::BOXH) {
+        if (threadIdx.x == 0) {
             s_xx[sj * G::BOXW + si] = fadd(s_xx[sj * G::BOXW + si], src_w);
             s_zz[sj * G::BOXW + si] = fadd(s_zz[sj * G::BOXW + si], src_w);
         }
+        __syncthreads();
     }
-    __syncthreads();
 
     const int cg = threadIdx.x % kCG, rp = threadIdx.x / kCG;
     const int x = x0 + 4 * cg, zt = z0 + 2 * rp;

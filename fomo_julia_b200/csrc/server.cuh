@@ -128,10 +128,12 @@ struct TuneKey {
         return std::tie(nx, nz, M, shots_log2) < std::tie(o.nx, o.nz, o.M, o.shots_log2);
     }
 };
+constexpr int kTuneSamples = 2;  // chunks timed per candidate (the fastest counts)
 struct TuneEntry {
     // device time per cell-step of the shots in flight (ms per Gcell-step):
-    // comparable across chunks whose shots differ
+    // comparable across chunks whose shots differ; the lowest of the samples
     double ms_per_work[3] = {-1, -1, -1};
+    int samples[3] = {0, 0, 0};
     int chosen = -1;
 };
 std::mutex g_tune_mu;
@@ -841,7 +843,7 @@ class Server {
         TuneEntry& e = g_tune[key];
         if (e.chosen >= 0) return e.chosen;
         for (int c = 0; c < 3; ++c)
-            if (e.ms_per_work[c] < 0) {
+            if (e.samples[c] < kTuneSamples) {
                 bool pending = false;
                 for (auto& m : measures_)
                     if (!(m.key < key) && !(key < m.key) && m.cand == c) pending = true;
@@ -866,12 +868,14 @@ class Server {
             {
                 std::lock_guard<std::mutex> lk(g_tune_mu);
                 TuneEntry& e = g_tune[m.key];
-                e.ms_per_work[m.cand] = ms / m.work;
+                const double t = ms / m.work;
+                if (e.ms_per_work[m.cand] < 0 || t < e.ms_per_work[m.cand]) e.ms_per_work[m.cand] = t;
+                e.samples[m.cand] += 1;
                 bool all = true;
                 int best = 0;
                 for (int c = 0; c < 3; ++c) {
-                    if (e.ms_per_work[c] < 0) all = false;
-                    else if (e.ms_per_work[best] < 0 || e.ms_per_work[c] < e.ms_per_work[best]) best = c;
+                    if (e.samples[c] < kTuneSamples) all = false;
+                    if (e.ms_per_work[c] >= 0 && (e.ms_per_work[best] < 0 || e.ms_per_work[c] < e.ms_per_work[best])) best = c;
                 }
                 if (all && e.chosen < 0) {
                     e.chosen = best;

@@ -12,8 +12,10 @@
 //                            its rules read lie in one tile, as the left band
 //                            does in the first tile.
 //       fast tiles: the stencil fields of the tile plus an M-cell halo and
-//         the tile's pointwise operands arrive by TMA (cp.async.bulk.tensor.2d,
-//         one mbarrier); each thread owns 4 columns x 2 rows, forms
+//         the tile's pointwise operands arrive by TMA (cp.async.bulk.tensor.2d;
+//         one mbarrier for the halo boxes, one for the tile boxes; each tile
+//         also prefetches into L2 the boxes of the tile kPrefetchAhead blocks
+//         later); each thread owns 4 columns x 2 rows, forms
 //         x-derivatives from 128-bit shared-memory row windows and
 //         z-derivatives from a (2M+1)-row register window.  Tiles
 //         holding left/right HABC cells park their stencil values in shared
@@ -149,6 +151,12 @@ __device__ __forceinline__ void tma_load_2d(float* dst, const CUtensorMap* map, 
         "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
         ::"r"(smem_u32(dst)), "l"((uint64_t)map), "r"(x), "r"(z), "r"(smem_u32(bar))
         : "memory");
+}
+
+// L2 prefetch of a box (nothing reaches shared memory, nothing to wait for).
+__device__ __forceinline__ void tma_prefetch_2d(const CUtensorMap* map, int x, int z) {
+    asm volatile("cp.async.bulk.prefetch.tensor.2d.L2.global.tile [%0, {%1, %2}];" ::"l"((uint64_t)map), "r"(x), "r"(z)
+                 : "memory");
 }
 
 // 4-byte asynchronous global -> shared copy; valid == false writes zero.
@@ -419,9 +427,17 @@ struct TilePre {
     __device__ float operator()(int i, int j) const { return spre[(f * kTZ + (j - z0)) * kTX + (i - x0)]; }
 };
 
+// L2 prefetch of the boxes of tile `tile` when it is a fast tile of this
+// launch (single-shot launches: the tile one wave of blocks ahead, so its
+// DRAM reads start while this tile is computed; defined after classify).
+template <int M>
+__device__ void prefetch_vel(const StepParams& P, const TiledArgs& T, const VelMapRefs& mp, int tile);
+template <int M>
+__device__ void prefetch_str(const StepParams& P, const TiledArgs& T, const StrMapRefs& mp, int tile);
+
 template <int M>
 __device__ __forceinline__ void fast_vel(const StepParams& P, const TiledArgs& T, const VelMapRefs& mp, int x0, int z0,
-                                         int x_end, bool band, bool rim, float* smem, float src_w) {
+                                         int x_end, bool band, bool rim, float* smem, float src_w, int pf_tile = -1) {
     using G = Geo<M>;
     constexpr int BOX = G::BOXS;
     float* s_xx = smem;
@@ -455,6 +471,7 @@ __device__ __forceinline__ void fast_vel(const StepParams& P, const TiledArgs& T
             tma_load_2d(p_b1, mp.b1, x0, z0, bar + 1);
             tma_load_2d(p_b3, mp.b3, x0, z0, bar + 1);
         }
+        if (pf_tile >= 0) prefetch_vel<M>(P, T, mp, pf_tile);
     }
     __syncthreads();
     if (!wait_tma(bar, T)) return;
@@ -548,7 +565,7 @@ __device__ __forceinline__ void fast_vel(const StepParams& P, const TiledArgs& T
 
 template <int M>
 __device__ __forceinline__ void fast_str(const StepParams& P, const TiledArgs& T, const StrMapRefs& mp, int x0, int z0,
-                                         int x_end, bool band, bool rim, float* smem, float src_w) {
+                                         int x_end, bool band, bool rim, float* smem, float src_w, int pf_tile = -1) {
     using G = Geo<M>;
     constexpr int BOX = G::BOXS;
     float* s_vx = smem;
@@ -575,6 +592,7 @@ __device__ __forceinline__ void fast_str(const StepParams& P, const TiledArgs& T
         tma_load_2d(p_lam, mp.lam, x0, z0, bar + 1);
         tma_load_2d(p_mu, mp.mu, x0, z0, bar + 1);
         tma_load_2d(p_mxz, mp.mxz, x0, z0, bar + 1);
+        if (pf_tile >= 0) prefetch_str<M>(P, T, mp, pf_tile);
     }
     __syncthreads();
     if (!wait_tma(bar, T)) return;
@@ -712,6 +730,47 @@ __device__ __forceinline__ bool reads_band_rows(const StepParams& P, int z0) {
     return z0 + kTZ + kEdgeZ + P.M >= P.nz - P.nbc - 1;
 }
 
+// How far ahead a tile prefetches: two tile blocks per SM.  Measured on the
+// 4552 x 3927 grid, the velocity launch was fastest 260-370 blocks ahead
+// (113.8 us at one wave, 740; 140.9 us at 1480) and the stress launch
+// 185-370 ahead (148.8 us at 92, 150 us at 740).
+constexpr int kPrefetchAhead = 2 * 148;
+
+template <int M>
+__device__ void prefetch_vel(const StepParams& P, const TiledArgs& T, const VelMapRefs& mp, int tile) {
+    if (tile >= T.n_tile_blocks) return;
+    const TileKind k = classify(P, T, tile);
+    if (k.generic) return;
+    using G = Geo<M>;
+    tma_prefetch_2d(mp.xx, k.x0 - G::HX, k.z0 - M);
+    tma_prefetch_2d(mp.zz, k.x0 - G::HX, k.z0 - M);
+    tma_prefetch_2d(mp.xz, k.x0 - G::HX, k.z0 - M);
+    tma_prefetch_2d(mp.vx, k.x0, k.z0);
+    tma_prefetch_2d(mp.vz, k.x0, k.z0);
+    tma_prefetch_2d(mp.b0, k.x0, k.z0);
+    tma_prefetch_2d(mp.b2, k.x0, k.z0);
+    if (!T.iso) {
+        tma_prefetch_2d(mp.b1, k.x0, k.z0);
+        tma_prefetch_2d(mp.b3, k.x0, k.z0);
+    }
+}
+
+template <int M>
+__device__ void prefetch_str(const StepParams& P, const TiledArgs& T, const StrMapRefs& mp, int tile) {
+    if (tile >= T.n_tile_blocks) return;
+    const TileKind k = classify(P, T, tile);
+    if (k.generic) return;
+    using G = Geo<M>;
+    tma_prefetch_2d(mp.vx, k.x0 - G::HX, k.z0 - M);
+    tma_prefetch_2d(mp.vz, k.x0 - G::HX, k.z0 - M);
+    tma_prefetch_2d(mp.txx, k.x0, k.z0);
+    tma_prefetch_2d(mp.tzz, k.x0, k.z0);
+    tma_prefetch_2d(mp.txz, k.x0, k.z0);
+    tma_prefetch_2d(mp.lam, k.x0, k.z0);
+    tma_prefetch_2d(mp.mu, k.x0, k.z0);
+    tma_prefetch_2d(mp.mxz, k.x0, k.z0);
+}
+
 // ---------------------------------------------------------------- receivers
 // rec_k: 1-based step recorded from P.in (P.rec_k on the single-shot path).
 __device__ inline void record_block(const StepParams& P, int rblock, int rec_k) {
@@ -735,7 +794,7 @@ __global__ void __launch_bounds__(kThreads, kTileBlocks<M>) velocity_kernel(cons
         const TileKind k = classify(P, T, bid);
         if (reads_band_rows(P, k.z0)) grid_dep_wait();
         if (k.generic) edge_tile<M, true>(P, T, k.x0, k.z0, k.x_end, smem, P.src_w);
-        else fast_vel<M>(P, T, refs_of(maps), k.x0, k.z0, k.x_end, k.band, k.rim, smem, P.src_w);
+        else fast_vel<M>(P, T, refs_of(maps), k.x0, k.z0, k.x_end, k.band, k.rim, smem, P.src_w, bid + kPrefetchAhead);
         return;
     }
     grid_dep_wait();  // receivers may sit in the band rows
@@ -751,7 +810,7 @@ __global__ void __launch_bounds__(kThreads, kTileBlocks<M>) stress_kernel(const 
         const TileKind k = classify(P, T, bid);
         if (reads_band_rows(P, k.z0)) grid_dep_wait();
         if (k.generic) edge_tile<M, false>(P, T, k.x0, k.z0, k.x_end, smem, P.src_w);
-        else fast_str<M>(P, T, refs_of(maps), k.x0, k.z0, k.x_end, k.band, k.rim, smem, P.src_w);
+        else fast_str<M>(P, T, refs_of(maps), k.x0, k.z0, k.x_end, k.band, k.rim, smem, P.src_w, bid + kPrefetchAhead);
     }
 }
 

@@ -129,6 +129,11 @@ struct TuneKey {
     }
 };
 constexpr int kTuneSamples = 2;  // chunks timed per candidate (the fastest counts)
+// Candidates the autotuner times: graphs of 8 and of 32 steps.  Plain
+// launches (kTuneK[0]) run only when configured: over the bench's batched,
+// uneven and serving runs the tuner never chose them, and their timed chunks
+// are the slowest of a short mixed run.
+constexpr int kTuneFirst = 1;
 struct TuneEntry {
     // device time per cell-step of the shots in flight (ms per Gcell-step):
     // comparable across chunks whose shots differ; the lowest of the samples
@@ -842,7 +847,7 @@ class Server {
         std::lock_guard<std::mutex> lk(g_tune_mu);
         TuneEntry& e = g_tune[key];
         if (e.chosen >= 0) return e.chosen;
-        for (int c = 0; c < 3; ++c)
+        for (int c = kTuneFirst; c < 3; ++c)
             if (e.samples[c] < kTuneSamples) {
                 bool pending = false;
                 for (auto& m : measures_)
@@ -872,8 +877,8 @@ class Server {
                 if (e.ms_per_work[m.cand] < 0 || t < e.ms_per_work[m.cand]) e.ms_per_work[m.cand] = t;
                 e.samples[m.cand] += 1;
                 bool all = true;
-                int best = 0;
-                for (int c = 0; c < 3; ++c) {
+                int best = kTuneFirst;
+                for (int c = kTuneFirst; c < 3; ++c) {
                     if (e.samples[c] < kTuneSamples) all = false;
                     if (e.ms_per_work[c] >= 0 && (e.ms_per_work[best] < 0 || e.ms_per_work[c] < e.ms_per_work[best])) best = c;
                 }

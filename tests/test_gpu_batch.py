@@ -269,7 +269,7 @@ def test_tune_cache_file(b200, tmp_path, monkeypatch):
     monkeypatch.setenv("FOMO_B200_TUNE_CACHE", str(path))
     c = layered(97, 61, seed=8, nbc=6, fd_order=8, nt=400)
     S = setup(c, b200)
-    with F.ShotServer() as srv:  # autotuned K: the three candidates are measured on live chunks
+    with F.ShotServer() as srv:  # autotuned K: the candidates are timed on live chunks
         srv.wait_all([srv.submit(S.med, S.H, S.a, source(S, 100.0 + 30 * k, 20.0), S.rec, params_of(S))
                       for k in range(3)], timeout=WAIT_S)
     lines = path.read_text().split("\n")

@@ -428,8 +428,9 @@ struct TilePre {
 };
 
 // L2 prefetch of the boxes of tile `tile` when it is a fast tile of this
-// launch (single-shot launches: the tile one wave of blocks ahead, so its
-// DRAM reads start while this tile is computed; defined after classify).
+// launch (defined after classify).  The single-shot fast tiles pass
+// pf_tile = their block + kPrefetchAhead, so that tile's DRAM reads start
+// while this one is computed; the batched launches pass -1 (no prefetch).
 template <int M>
 __device__ void prefetch_vel(const StepParams& P, const TiledArgs& T, const VelMapRefs& mp, int tile);
 template <int M>

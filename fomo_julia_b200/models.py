@@ -6,9 +6,12 @@
   dtype Float32 by default; order column-major (x fastest) or row-major.
   vs and rho come from files, from arrays, or are estimated from vp.
 * ``.npy``: NumPy arrays (model_loader.jl:288-320).
-* ``.jld2``, ``.segy``/``.sgy``, ``.mat``, ``.h5``/``.hdf5`` need Julia or
-  libraries not present here.  They raise NotImplementedError naming the
-  format; convert such models to .bin or .npy first.
+* ``.segy``/``.sgy``: SEG-Y (model_loader.jl:199-248, which reads through
+  SegyIO.jl's segy_read and takes its data matrix, samples x traces, as vp).
+  Read here without SegyIO: ``read_segy`` below.
+* ``.jld2``, ``.mat``, ``.h5``/``.hdf5`` need Julia or libraries not present
+  here.  They raise NotImplementedError naming the format; convert such
+  models to .bin, .npy or SEG-Y first.
 
 Estimates as in the reference: vs = vp / 1.73 and rho = 310 vp^0.25 (Gardner),
 in Float32.  numpy's float32 power may differ from Julia's in the last bit;
@@ -83,10 +86,115 @@ def _other(v, reader, vp, estimate):
     return np.asarray(v)
 
 
+# ---------------------------------------------------------------- SEG-Y
+# Layout (SEG-Y rev 0/1, big-endian): a 3200-byte textual header, a 400-byte
+# binary header (samples per trace at byte 20, sample format code at byte 24,
+# count of extended 3200-byte textual headers at byte 304), then traces of a
+# 240-byte trace header and the samples.  Format codes: 1 IBM 4-byte float,
+# 2 int32, 3 int16, 5 IEEE 4-byte float, 8 int8.
+_SEGY_TEXT, _SEGY_BIN, _SEGY_TRACE_HDR = 3200, 400, 240
+_SEGY_FORMATS = {1: ">u4", 2: ">i4", 3: ">i2", 5: ">f4", 8: "i1"}
+
+
+def ibm_to_float32(words) -> np.ndarray:
+    """IBM System/360 single-precision floats (32-bit words) to float32.
+
+    An IBM float is sign s, 7-bit excess-64 exponent e and 24-bit fraction f:
+    (-1)^s * (f / 2^24) * 16^(e - 64).  That value is exact in float64 and
+    rounded once to float32 (values beyond float32's range become inf or
+    round to zero or a subnormal)."""
+    w = np.asarray(words, dtype=np.uint32)
+    sign = np.where(w >> 31, -1.0, 1.0)
+    expo = ((w >> 24) & 0x7F).astype(np.int64) - 64
+    frac = (w & 0x00FFFFFF).astype(np.float64) / float(1 << 24)
+    with np.errstate(over="ignore", under="ignore"):
+        return (sign * np.ldexp(frac, 4 * expo)).astype(np.float32)
+
+
+def float32_to_ibm(values) -> np.ndarray:
+    """float32 to IBM single-precision words (the inverse of ibm_to_float32
+    for values IBM can hold; the 24-bit fraction truncates, as IBM
+    arithmetic does).  Zero maps to 0."""
+    v = np.asarray(values, dtype=np.float64)
+    out = np.zeros(v.shape, dtype=np.uint32)
+    nz = v != 0
+    a = np.abs(v[nz])
+    expo = np.floor(np.log2(a) / 4).astype(np.int64) + 1  # a = frac * 16^expo with frac in [1/16, 1)
+    frac = a / np.ldexp(1.0, 4 * expo)
+    hi = frac >= 1.0                                      # guard the log2 rounding at powers of 16
+    expo[hi] += 1
+    frac[hi] /= 16.0
+    lo = frac < 1.0 / 16
+    expo[lo] -= 1
+    frac[lo] *= 16.0
+    f24 = np.floor(frac * (1 << 24)).astype(np.uint64)
+    words = (np.where(v[nz] < 0, 1, 0).astype(np.uint64) << 31) | (((expo + 64) & 0x7F).astype(np.uint64) << 24) | f24
+    out[nz] = words.astype(np.uint32)
+    return out
+
+
+def read_segy(path: str) -> np.ndarray:
+    """The data matrix of a SEG-Y file as float32, samples x traces (the
+    orientation of SegyIO's SeisBlock.data), for fixed-length traces."""
+    raw = np.fromfile(path, dtype=np.uint8)
+    if raw.size < _SEGY_TEXT + _SEGY_BIN:
+        raise ValueError(f"{path}: {raw.size} bytes, too short for a SEG-Y file")
+    bh = raw[_SEGY_TEXT:_SEGY_TEXT + _SEGY_BIN]
+    ns = int(bh[20:22].view(">u2")[0])
+    fmt = int(bh[24:26].view(">u2")[0])
+    n_ext = int(bh[304:306].view(">i2")[0])
+    if fmt not in _SEGY_FORMATS:
+        raise ValueError(f"{path}: sample format code {fmt} not supported (1, 2, 3, 5, 8)")
+    if ns <= 0:
+        raise ValueError(f"{path}: {ns} samples per trace in the binary header")
+    dt = np.dtype(_SEGY_FORMATS[fmt])
+    start = _SEGY_TEXT + _SEGY_BIN + max(n_ext, 0) * _SEGY_TEXT
+    trace_bytes = _SEGY_TRACE_HDR + ns * dt.itemsize
+    body = raw.size - start
+    if body < 0 or body % trace_bytes:
+        raise ValueError(f"{path}: {body} bytes of traces is not a whole number of "
+                         f"{trace_bytes}-byte traces (variable-length traces are not supported)")
+    n_tr = body // trace_bytes
+    traces = raw[start:].reshape(n_tr, trace_bytes)[:, _SEGY_TRACE_HDR:]
+    samples = np.ascontiguousarray(traces).view(dt).reshape(n_tr, ns)
+    data = ibm_to_float32(samples) if fmt == 1 else samples.astype(np.float32)
+    return np.asfortranarray(data.T)
+
+
+def write_segy(path: str, data, fmt: int = 5, sample_interval_us: int = 0) -> None:
+    """Writes `data` (samples x traces) as a SEG-Y rev 1 file with IEEE
+    (fmt 5) or IBM (fmt 1) 4-byte floats: blank EBCDIC textual header,
+    binary header with the sample count and format, minimal trace headers."""
+    if fmt not in (1, 5):
+        raise ValueError("fmt must be 1 (IBM) or 5 (IEEE)")
+    d = np.asarray(data, dtype=np.float32)
+    if d.ndim != 2:
+        raise ValueError("data must be a 2-D samples x traces array")
+    ns, n_tr = d.shape
+    text = np.full(_SEGY_TEXT, 0x40, dtype=np.uint8)  # EBCDIC spaces
+    bh = np.zeros(_SEGY_BIN, dtype=np.uint8)
+    bh[16:18] = np.array([sample_interval_us], dtype=">u2").view(np.uint8)
+    bh[20:22] = np.array([ns], dtype=">u2").view(np.uint8)
+    bh[24:26] = np.array([fmt], dtype=">u2").view(np.uint8)
+    bh[300:302] = np.array([0x0100], dtype=">u2").view(np.uint8)  # revision 1
+    bh[302:304] = np.array([1], dtype=">u2").view(np.uint8)       # fixed-length traces
+    hdr = np.zeros((n_tr, _SEGY_TRACE_HDR), dtype=np.uint8)
+    hdr[:, 0:4] = np.arange(1, n_tr + 1, dtype=">i4").view(np.uint8).reshape(n_tr, 4)  # trace sequence number
+    hdr[:, 114:116] = np.array([ns], dtype=">u2").view(np.uint8)
+    hdr[:, 116:118] = np.array([sample_interval_us], dtype=">u2").view(np.uint8)
+    cols = d.T  # traces x samples
+    body = float32_to_ibm(cols).astype(">u4") if fmt == 1 else cols.astype(">f4")
+    traces = np.concatenate([hdr, np.ascontiguousarray(body).view(np.uint8).reshape(n_tr, 4 * ns)], axis=1)
+    with open(path, "wb") as f:
+        f.write(text.tobytes())
+        f.write(bh.tobytes())
+        f.write(traces.tobytes())
+
+
 def load_model(path: str, nx: Optional[int] = None, nz: Optional[int] = None, dx=1.0, dz=None,
                dtype=np.float32, order: str = "column_major", vs=None, rho=None, single: bool = False
                ) -> Union[VelocityModel, np.ndarray]:
-    """load_model (model_loader.jl:88-106) for .bin and .npy files."""
+    """load_model (model_loader.jl:88-106) for .bin, .npy and SEG-Y files."""
     ext = os.path.splitext(path)[1].lower()
     dz = dx if dz is None else dz
     if ext == ".bin":
@@ -95,8 +203,13 @@ def load_model(path: str, nx: Optional[int] = None, nz: Optional[int] = None, dx
         read = lambda p: _read_bin(p, int(nx), int(nz), dtype, order)  # noqa: E731
     elif ext == ".npy":
         read = lambda p: np.asfortranarray(np.load(p).astype(f32))  # noqa: E731
-    elif ext in (".jld2", ".segy", ".sgy", ".mat", ".h5", ".hdf5"):
-        raise NotImplementedError(f"{ext} models need Julia or a library absent here; convert to .bin or .npy")
+    elif ext in (".segy", ".sgy"):
+        def read(p):
+            if not str(p).lower().endswith((".segy", ".sgy")):  # model_loader.jl:229-245 reads only SEG-Y paths
+                raise ValueError(f"{p}: vs and rho of a SEG-Y model must be SEG-Y files or arrays")
+            return read_segy(p)
+    elif ext in (".jld2", ".mat", ".h5", ".hdf5"):
+        raise NotImplementedError(f"{ext} models need Julia or a library absent here; convert to .bin, .npy or SEG-Y")
     else:
         raise ValueError(f"Unsupported format: {ext}\nSupported: .jld2, .segy, .sgy, .bin, .mat, .npy, .h5, .hdf5")
     vp = read(path)

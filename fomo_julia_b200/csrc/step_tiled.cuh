@@ -802,16 +802,30 @@ __global__ void __launch_bounds__(kThreads, kTileBlocks<M>) velocity_kernel(cons
     record_block(P, bid - T.n_tile_blocks, P.rec_k);
 }
 
+// Tile of stress block b.  The velocity launch before it ran top to bottom,
+// so the last rows it read and wrote are the ones still in L2; the stress
+// launch takes the tile rows that do not wait for the band pass in reverse
+// raster order (bottom-right first), then the rows that read the band rows
+// (they wait for the band pass) in raster order.  Blocks b >= the tile count
+// map to themselves.
+__device__ __forceinline__ int stress_tile(const StepParams& P, const TiledArgs& T, int b) {
+    const int lim = P.nz - P.nbc - 1 - kTZ - kEdgeZ - P.M;  // a tile with z0 >= lim reads band rows
+    const int tz_wait = lim <= 0 ? 0 : (lim + kTZ - 1) / kTZ;
+    const int n_early = min(tz_wait * T.tiles_x, T.n_tile_blocks);
+    return b < n_early ? n_early - 1 - b : b;
+}
+
 template <int M>
 __global__ void __launch_bounds__(kThreads, kTileBlocks<M>) stress_kernel(const __grid_constant__ StepParams P, const __grid_constant__ TiledArgs T,
                                                           const __grid_constant__ StrMaps maps) {
     extern __shared__ __align__(128) float smem[];
     const int bid = blockIdx.x;
     if (bid < T.n_tile_blocks) {
-        const TileKind k = classify(P, T, bid);
+        const TileKind k = classify(P, T, stress_tile(P, T, bid));
         if (reads_band_rows(P, k.z0)) grid_dep_wait();
         if (k.generic) edge_tile<M, false>(P, T, k.x0, k.z0, k.x_end, smem, P.src_w);
-        else fast_str<M>(P, T, refs_of(maps), k.x0, k.z0, k.x_end, k.band, k.rim, smem, P.src_w, bid + kPrefetchAhead);
+        else fast_str<M>(P, T, refs_of(maps), k.x0, k.z0, k.x_end, k.band, k.rim, smem, P.src_w,
+                         stress_tile(P, T, bid + kPrefetchAhead));
     }
 }
 

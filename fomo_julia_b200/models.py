@@ -9,9 +9,13 @@
 * ``.segy``/``.sgy``: SEG-Y (model_loader.jl:199-248, which reads through
   SegyIO.jl's segy_read and takes its data matrix, samples x traces, as vp).
   Read here without SegyIO: ``read_segy`` below.
-* ``.jld2``, ``.mat``, ``.h5``/``.hdf5`` need Julia or libraries not present
-  here.  They raise NotImplementedError naming the format; convert such
-  models to .bin, .npy or SEG-Y first.
+* ``.mat``: MATLAB v4/v5 files through scipy.io.loadmat (model_loader.jl:
+  254-283: vp under vp_key, "Vp" or "VP"; vs under vs_key or "Vs"; rho under
+  rho_key, "Rho" or "density"; missing vs and rho estimated).  v7.3 files are
+  HDF5 and need a reader absent here.
+* ``.jld2``, ``.h5``/``.hdf5`` need Julia or libraries not present here.
+  They raise NotImplementedError naming the format; convert such models to
+  .bin, .npy, SEG-Y or MAT v5 first.
 
 Estimates as in the reference: vs = vp / 1.73 and rho = 310 vp^0.25 (Gardner),
 in Float32.  numpy's float32 power may differ from Julia's in the last bit;
@@ -191,12 +195,41 @@ def write_segy(path: str, data, fmt: int = 5, sample_interval_us: int = 0) -> No
         f.write(traces.tobytes())
 
 
+def _load_mat(path: str, vp_key: str, vs_key: str, rho_key: str, dx, dz) -> VelocityModel:
+    """_load_mat (model_loader.jl:254-283) for MATLAB v4/v5 files."""
+    from scipy.io import loadmat
+    try:
+        data = loadmat(path)
+    except NotImplementedError as e:  # scipy's answer to v7.3 (HDF5) files
+        raise NotImplementedError(f"{path}: MATLAB v7.3 files are HDF5, and no HDF5 reader is present here; "
+                                  f"save the model with -v7 or convert it to .bin, .npy or SEG-Y") from e
+
+    def pick(*keys):
+        for k in keys:
+            if k in data:
+                return data[k]
+        return None
+
+    vp = pick(vp_key, "Vp", "VP")
+    if vp is None:
+        raise ValueError(f"Cannot find vp field. Available keys: {sorted(k for k in data if not k.startswith('__'))}")
+    vp = np.asfortranarray(np.asarray(vp).astype(f32))
+    vs = pick(vs_key, "Vs")
+    rho = pick(rho_key, "Rho", "density")
+    vs = estimate_vs(vp) if vs is None else np.asarray(vs).astype(f32)
+    rho = gardner_rho(vp) if rho is None else np.asarray(rho).astype(f32)
+    return VelocityModel.make(vp, vs, rho, dx, dz, name=os.path.basename(path))
+
+
 def load_model(path: str, nx: Optional[int] = None, nz: Optional[int] = None, dx=1.0, dz=None,
-               dtype=np.float32, order: str = "column_major", vs=None, rho=None, single: bool = False
-               ) -> Union[VelocityModel, np.ndarray]:
-    """load_model (model_loader.jl:88-106) for .bin, .npy and SEG-Y files."""
+               dtype=np.float32, order: str = "column_major", vs=None, rho=None, single: bool = False,
+               vp_key: str = "vp", vs_key: str = "vs", rho_key: str = "rho") -> Union[VelocityModel, np.ndarray]:
+    """load_model (model_loader.jl:88-106) for .bin, .npy, SEG-Y and MAT v4/v5 files."""
     ext = os.path.splitext(path)[1].lower()
     dz = dx if dz is None else dz
+    if ext == ".mat":
+        m = _load_mat(path, vp_key, vs_key, rho_key, dx, dz)
+        return m.vp if single else m
     if ext == ".bin":
         if nx is None or nz is None:
             raise ValueError("Binary files require nx and nz parameters")
@@ -208,8 +241,9 @@ def load_model(path: str, nx: Optional[int] = None, nz: Optional[int] = None, dx
             if not str(p).lower().endswith((".segy", ".sgy")):  # model_loader.jl:229-245 reads only SEG-Y paths
                 raise ValueError(f"{p}: vs and rho of a SEG-Y model must be SEG-Y files or arrays")
             return read_segy(p)
-    elif ext in (".jld2", ".mat", ".h5", ".hdf5"):
-        raise NotImplementedError(f"{ext} models need Julia or a library absent here; convert to .bin, .npy or SEG-Y")
+    elif ext in (".jld2", ".h5", ".hdf5"):
+        raise NotImplementedError(f"{ext} models need Julia or a library absent here; "
+                                  f"convert to .bin, .npy, SEG-Y or MAT v5")
     else:
         raise ValueError(f"Unsupported format: {ext}\nSupported: .jld2, .segy, .sgy, .bin, .mat, .npy, .h5, .hdf5")
     vp = read(path)

@@ -45,7 +45,7 @@ def test_npy_and_unsupported(tmp_path):
     got = models.load_model(str(tmp_path / "vp.npy"), vs=str(tmp_path / "vs.npy"), rho=str(tmp_path / "rho.npy"),
                             dx=10.0, dz=12.5)
     assert np.array_equal(got.rho, m.rho) and got.name == "vp.npy"
-    for ext in (".jld2", ".mat", ".h5"):
+    for ext in (".jld2", ".h5"):
         with pytest.raises(NotImplementedError):
             models.load_model(str(tmp_path / f"x{ext}"))
     with pytest.raises(ValueError):
@@ -114,3 +114,25 @@ def test_load_model_segy(tmp_path):
     np.save(tmp_path / "vs.npy", vs)
     with pytest.raises(ValueError):
         models.load_model(str(tmp_path / "vp.segy"), vs=str(tmp_path / "vs.npy"))
+
+
+# ---------------------------------------------------------------- MAT
+def test_load_model_mat(tmp_path):
+    from scipy.io import savemat
+    rng = np.random.default_rng(5)
+    vp = rng.uniform(1500.0, 4500.0, (12, 9))            # float64, as MATLAB saves
+    vs = vp / 1.8
+    rho = np.full_like(vp, 2150.25)
+    savemat(str(tmp_path / "a.mat"), {"Vp": vp, "Vs": vs, "density": rho})
+    m = models.load_model(str(tmp_path / "a.mat"), dx=5.0)
+    assert (m.nx, m.nz) == (12, 9) and m.dx == m.dz == np.float32(5.0) and m.name == "a.mat"
+    assert np.array_equal(m.vp, vp.astype(np.float32)) and np.array_equal(m.vs, vs.astype(np.float32))
+    assert np.array_equal(m.rho, rho.astype(np.float32))
+    # only vp, under a custom key: vs and rho estimated as for the other formats
+    savemat(str(tmp_path / "b.mat"), {"velocity": vp})
+    m2 = models.load_model(str(tmp_path / "b.mat"), vp_key="velocity")
+    v32 = vp.astype(np.float32)
+    assert np.array_equal(m2.vs, v32 / np.float32(1.73)) and np.array_equal(m2.rho, models.gardner_rho(v32))
+    assert np.array_equal(models.load_model(str(tmp_path / "b.mat"), vp_key="velocity", single=True), v32)
+    with pytest.raises(ValueError):
+        models.load_model(str(tmp_path / "b.mat"))       # no vp, Vp or VP

@@ -124,7 +124,7 @@ def host_inputs(w):
     lam, mu, mu_txz, rho_vx, rho_vz = F.compute_staggered_params(
         F.pad_array(w.vp, pad), F.pad_array(w.vs, pad), F.pad_array(w.rho, pad))
     nx, nz = w.nx_in + 2 * pad, w.nz_in + 2 * pad
-    v_ref = F.julia_mean(w.vp) if w.vp.size <= 4_000_000 else np.float32(w.vp.mean(dtype=np.float64))
+    v_ref = F.julia_mean(w.vp)  # mean(vp), run.jl:57
     habc = F.init_habc(nx, nz, w.nbc, w.dt, w.dx, w.dz, v_ref)
     habc_v_ref = v_ref
     params = F.sim_params(w.dt, w.nt, w.dx, w.dz, w.fd_order)

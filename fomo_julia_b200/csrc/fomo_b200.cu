@@ -183,6 +183,47 @@ int ensure_init() {
     return FOMO_OK;
 }
 
+// SM count of the current device (grid sizes of the grid-stride kernels and
+// the tile prefetch distance scale with it); 148 if the query fails.
+int sm_count() {
+    static std::mutex mu;
+    static std::unordered_map<int, int> by_dev;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) {
+        (void)cudaGetLastError();
+        return 148;
+    }
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = by_dev.find(dev);
+    if (it != by_dev.end()) return it->second;
+    int n = 0;
+    if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) {
+        (void)cudaGetLastError();
+        n = 148;
+    }
+    by_dev[dev] = n;
+    return n;
+}
+
+// Raises a kernel's dynamic shared-memory limit on the current device to at
+// least `bytes` and never lowers it, so a launch sized by another caller for
+// a larger block stays valid.  One high-water mark per (kernel, device).
+template <class K>
+int raise_smem_limit(K* kernel, size_t bytes) {
+    static std::mutex mu;
+    static std::unordered_map<uint64_t, size_t> set;
+    if (bytes <= 48 * 1024) return FOMO_OK;
+    int dev = 0;
+    CUDA_TRY(cudaGetDevice(&dev));
+    const uint64_t key = (uint64_t)(uintptr_t)(const void*)kernel * 64 + (uint64_t)dev;
+    std::lock_guard<std::mutex> lk(mu);
+    size_t& cur = set[key];
+    if (bytes <= cur) return FOMO_OK;
+    CUDA_TRY(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+    cur = bytes;
+    return FOMO_OK;
+}
+
 // The HABC band must fit the grid, and the free-surface rows (pad-5..pad,
 // 0-based) must lie above the bottom band and the row above it.
 int check_band(int nx, int nz, int pad, int fs, int nbc) {
@@ -263,7 +304,7 @@ int ensure_buoyancy(Medium& m, float dtx, float dtz) {
     float* b1 = dtx == dtz ? b0 : m.buoy + plane;
     float* b2 = m.buoy + 2 * plane;
     float* b3 = dtx == dtz ? b2 : m.buoy + 3 * plane;
-    fomo::buoyancy_kernel<<<4 * 148, 256, 0, ctx().stream>>>(m.arr(0), m.arr(1), dtx, dtz, plane, b0, b1, b2, b3);
+    fomo::buoyancy_kernel<<<4 * sm_count(), 256, 0, ctx().stream>>>(m.arr(0), m.arr(1), dtx, dtz, plane, b0, b1, b2, b3);
     CUDA_TRY(cudaGetLastError());
     m.buoy_dtx = dtx;
     m.buoy_dtz = dtz;
@@ -384,15 +425,8 @@ int run_steps_M(Shot& s, Medium& m, Wavefield& w, int n_steps, Profile* prof) {
     auto& C = ctx();
     const bool iso = s.dtx == s.dtz;
     const Launch L = launch_shape<M>(m.nx, m.nz, s.nbc, iso, m.fs != 0);
-    static size_t smem_set_v = 48 * 1024, smem_set_s = 48 * 1024;
-    if (L.smem_v > smem_set_v) {
-        CUDA_TRY(cudaFuncSetAttribute(fomo::velocity_kernel<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.smem_v));
-        smem_set_v = L.smem_v;
-    }
-    if (L.smem_s > smem_set_s) {
-        CUDA_TRY(cudaFuncSetAttribute(fomo::stress_kernel<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.smem_s));
-        smem_set_s = L.smem_s;
-    }
+    if (int rc = raise_smem_limit(fomo::velocity_kernel<M>, L.smem_v)) return rc;
+    if (int rc = raise_smem_limit(fomo::stress_kernel<M>, L.smem_s)) return rc;
     if (w.map_M != M)
         if (int rc = make_maps<M>(w)) return rc;
     if (int rc = ensure_buoyancy(m, s.dtx, s.dtz)) return rc;
@@ -405,6 +439,7 @@ int run_steps_M(Shot& s, Medium& m, Wavefield& w, int n_steps, Profile* prof) {
     T.n_tile_blocks = L.n_tile;
     T.tiles_x = L.tiles_x;
     T.x_last = L.x_last;
+    T.prefetch_ahead = fomo::prefetch_distance(sm_count());
     const int rec_blocks = (s.n_rec + fomo::kThreads - 1) / fomo::kThreads;
     CUDA_TRY(cudaEventRecord(C.ev0, C.stream));
     const int k_begin = s.k_done + 1, k_end = std::min(s.nt, s.k_done + n_steps);
@@ -711,7 +746,7 @@ int fomo_b200_medium_create_from_model(int32_t nx_in, int32_t nz_in, const float
             rc = fail(FOMO_ECUDA, "model upload failed");
     if (rc == FOMO_OK) {
         fomo::ModelView V{d_model, d_model + model, d_model + 2 * model, nx_in, nz_in, pad};
-        fomo::medium_init_kernel<<<8 * 148, 256, 0, st>>>(V, nx, nz, m->pitch, m->base, m->base + plane,
+        fomo::medium_init_kernel<<<8 * sm_count(), 256, 0, st>>>(V, nx, nz, m->pitch, m->base, m->base + plane,
                                                           m->base + 2 * plane, m->base + 3 * plane, m->base + 4 * plane);
         if (cudaGetLastError() != cudaSuccess) rc = fail(FOMO_ECUDA, "medium set-up kernel launch failed");
     }
@@ -832,7 +867,7 @@ int fomo_b200_wavefield_snapshot(uint64_t wavefield, int32_t kind, int32_t downs
     const int c = w->cur;
     const float* f0 = kind == 0 ? w->field(c, fomo::TXX) : kind == 3 ? w->field(c, fomo::VZ) : w->field(c, fomo::VX);
     const float* f1 = kind == 0 ? w->field(c, fomo::TZZ) : w->field(c, fomo::VZ);
-    fomo::snapshot_kernel<<<4 * 148, 256, 0, ctx().stream>>>(f0, f1, kind, w->nx, w->nz, w->pitch, downsample, nx_d,
+    fomo::snapshot_kernel<<<4 * sm_count(), 256, 0, ctx().stream>>>(f0, f1, kind, w->nx, w->nz, w->pitch, downsample, nx_d,
                                                              nz_d, w->snap);
     CUDA_TRY(cudaGetLastError());
     CUDA_TRY(cudaMemcpyAsync(host, w->snap, bytes, cudaMemcpyDeviceToHost, ctx().stream));
@@ -1021,10 +1056,9 @@ int fomo_b200_run_shot(uint64_t medium, uint64_t wavefield, const FomoHabc* habc
 // ---------------------------------------------------------------------------
 // Allocation-free shot: fomo_b200_run_shot_noalloc.
 //
-// Some callers cannot call cudaMalloc while they run a shot: a caller that is
-// capturing its stream into a CUDA graph (allocation is not a capturable
-// operation), a serving loop whose memory is carved once from a fixed pool at
-// start-up, or a host framework that forbids device allocation (and the
+// Some callers cannot call cudaMalloc while they run a shot: a serving loop
+// whose memory is carved once from a fixed pool at start-up and must not run
+// out later, or a host framework that forbids device allocation (and the
 // device-wide synchronisation cudaFree implies) on its latency path.  For them
 // this entry point runs the same time-step kernels with every scratch buffer
 // taken from one static device array: the two wavefield copies, the buoyancy
@@ -1037,7 +1071,9 @@ int fomo_b200_run_shot(uint64_t medium, uint64_t wavefield, const FomoHabc* habc
 // calls share it and it keeps the last call's contents: each call clears the
 // wavefield and the status word before its first step.  Calls that overlap on
 // the GPU (two streams, two threads, two devices' worth of work aimed at one
-// device) race on the array; callers must serialise them.
+// device) race on the array; callers must serialise them.  The first call on
+// a device resolves the array's address there (noalloc_scratch); it should
+// come before any stream capture on that device.
 // ---------------------------------------------------------------------------
 namespace {
 
@@ -1085,13 +1121,12 @@ int noalloc_loop(const fomo::StepParams& P0, fomo::TiledArgs T, float* fields, i
     for (int q = 0; q < 4; ++q)
         if (int rc = encode_map(&bm[q], buoy[q], nx, nz, pitch, fomo::kTX, fomo::kTZ)) return rc;
     const Launch L = launch_shape<M>(nx, nz, P0.nbc, iso, P0.fs != 0);
-    if (L.smem_v > 48 * 1024)
-        CUDA_TRY(cudaFuncSetAttribute(fomo::velocity_kernel<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.smem_v));
-    if (L.smem_s > 48 * 1024)
-        CUDA_TRY(cudaFuncSetAttribute(fomo::stress_kernel<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.smem_s));
+    if (int rc = raise_smem_limit(fomo::velocity_kernel<M>, L.smem_v)) return rc;
+    if (int rc = raise_smem_limit(fomo::stress_kernel<M>, L.smem_s)) return rc;
     T.n_tile_blocks = L.n_tile;
     T.tiles_x = L.tiles_x;
     T.x_last = L.x_last;
+    T.prefetch_ahead = fomo::prefetch_distance(sm_count());
     const int rec_blocks = (n_rec + fomo::kThreads - 1) / fomo::kThreads;
     int cur = 0;
     for (int k = 1; k <= nt; ++k) {
@@ -1210,7 +1245,7 @@ extern "C" int fomo_b200_run_shot_noalloc(int32_t nx, int32_t nz, int32_t M, int
     float* b2 = d_buo + pf;
     float* b1 = iso ? b0 : d_buo + 2 * pf;
     float* b3 = iso ? b2 : d_buo + 3 * pf;
-    fomo::buoyancy_kernel<<<4 * 148, 256, 0, st>>>(rho_vx, rho_vz, shot->dtx, shot->dtz, pf, b0, b1, b2, b3);
+    fomo::buoyancy_kernel<<<4 * sm_count(), 256, 0, st>>>(rho_vx, rho_vz, shot->dtx, shot->dtz, pf, b0, b1, b2, b3);
     CUDA_TRY(cudaGetLastError());
 
     fomo::StepParams P;

@@ -173,10 +173,6 @@ void save_tune_choice(const TuneKey& k, int cand) {
     }
 }
 
-// Largest dynamic shared memory set so far for the batch kernels, per M.
-std::mutex g_batch_attr_mu;
-size_t g_batch_smem[2][fomo::kMaxM + 1] = {};
-
 size_t batch_smem_any(int M, bool vel, int nbc, bool iso, bool fs) {
     switch (M) {
         case 1: return fomo::tiled_smem_bytes<1>(vel, nbc, iso, fs);
@@ -191,16 +187,8 @@ size_t batch_smem_any(int M, bool vel, int nbc, bool iso, bool fs) {
 
 template <int M>
 int set_batch_smem_M(size_t v, size_t s) {
-    std::lock_guard<std::mutex> lk(g_batch_attr_mu);
-    if (v > g_batch_smem[0][M] && v > 48 * 1024) {
-        CUDA_TRY(cudaFuncSetAttribute(fomo::batch_velocity_kernel<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)v));
-        g_batch_smem[0][M] = v;
-    }
-    if (s > g_batch_smem[1][M] && s > 48 * 1024) {
-        CUDA_TRY(cudaFuncSetAttribute(fomo::batch_stress_kernel<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s));
-        g_batch_smem[1][M] = s;
-    }
-    return FOMO_OK;
+    if (int rc = raise_smem_limit(fomo::batch_velocity_kernel<M>, v)) return rc;
+    return raise_smem_limit(fomo::batch_stress_kernel<M>, s);
 }
 
 int set_batch_smem(int M, size_t v, size_t s) {
@@ -515,7 +503,7 @@ class Server {
         float* b2 = R->buoy + plane;
         float* b1 = R->iso ? b0 : R->buoy + 2 * plane;
         float* b3 = R->iso ? b2 : R->buoy + 3 * plane;
-        fomo::buoyancy_kernel<<<4 * 148, 256, 0, st_>>>(m.arr(0), m.arr(1), r.dtx, r.dtz, plane, b0, b1, b2, b3);
+        fomo::buoyancy_kernel<<<4 * sm_count(), 256, 0, st_>>>(m.arr(0), m.arr(1), r.dtx, r.dtz, plane, b0, b1, b2, b3);
         if (cudaGetLastError() != cudaSuccess) {
             *rc = fail(FOMO_ECUDA, "buoyancy kernel launch failed");
             return nullptr;

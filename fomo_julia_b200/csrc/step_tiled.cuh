@@ -14,7 +14,7 @@
 //       fast tiles: the stencil fields of the tile plus an M-cell halo and
 //         the tile's pointwise operands arrive by TMA (cp.async.bulk.tensor.2d;
 //         one mbarrier for the halo boxes, one for the tile boxes; each tile
-//         also prefetches into L2 the boxes of the tile kPrefetchAhead blocks
+//         also prefetches into L2 the boxes of the tile prefetch_ahead blocks
 //         later); each thread owns 4 columns x 2 rows, forms
 //         x-derivatives from 128-bit shared-memory row windows and
 //         z-derivatives from a (2M+1)-row register window.  Tiles
@@ -70,6 +70,7 @@ struct TiledArgs {
     float* band_pre;     // pre-HABC values of the bottom band rows (see band_pre_at)
     int n_tile_blocks, tiles_x;
     int x_last;          // first column of the last tile of a row (a multiple of 4)
+    int prefetch_ahead;  // tile blocks between a fast tile and the tile it prefetches (0 = none)
 };
 
 __device__ __forceinline__ int tile_x0(const TiledArgs& T, int tx) {
@@ -429,7 +430,7 @@ struct TilePre {
 
 // L2 prefetch of the boxes of tile `tile` when it is a fast tile of this
 // launch (defined after classify).  The single-shot fast tiles pass
-// pf_tile = their block + kPrefetchAhead, so that tile's DRAM reads start
+// pf_tile = their block + T.prefetch_ahead, so that tile's DRAM reads start
 // while this one is computed; the batched launches pass -1 (no prefetch).
 template <int M>
 __device__ void prefetch_vel(const StepParams& P, const TiledArgs& T, const VelMapRefs& mp, int tile);
@@ -731,11 +732,12 @@ __device__ __forceinline__ bool reads_band_rows(const StepParams& P, int z0) {
     return z0 + kTZ + kEdgeZ + P.M >= P.nz - P.nbc - 1;
 }
 
-// How far ahead a tile prefetches: two tile blocks per SM.  Measured on the
-// 4552 x 3927 grid, the velocity launch was fastest 260-370 blocks ahead
-// (113.8 us at one wave, 740; 140.9 us at 1480) and the stress launch
+// How far ahead a tile prefetches (TiledArgs::prefetch_ahead): two tile
+// blocks per SM of the device (prefetch_distance).  Measured on the
+// 4552 x 3927 grid on 148 SMs, the velocity launch was fastest 260-370 blocks
+// ahead (113.8 us at one wave, 740; 140.9 us at 1480) and the stress launch
 // 185-370 ahead (148.8 us at 92, 150 us at 740).
-constexpr int kPrefetchAhead = 2 * 148;
+__host__ inline int prefetch_distance(int sm_count) { return 2 * sm_count; }
 
 template <int M>
 __device__ void prefetch_vel(const StepParams& P, const TiledArgs& T, const VelMapRefs& mp, int tile) {
@@ -795,7 +797,8 @@ __global__ void __launch_bounds__(kThreads, kTileBlocks<M>) velocity_kernel(cons
         const TileKind k = classify(P, T, bid);
         if (reads_band_rows(P, k.z0)) grid_dep_wait();
         if (k.generic) edge_tile<M, true>(P, T, k.x0, k.z0, k.x_end, smem, P.src_w);
-        else fast_vel<M>(P, T, refs_of(maps), k.x0, k.z0, k.x_end, k.band, k.rim, smem, P.src_w, bid + kPrefetchAhead);
+        else fast_vel<M>(P, T, refs_of(maps), k.x0, k.z0, k.x_end, k.band, k.rim, smem, P.src_w,
+                         T.prefetch_ahead > 0 ? bid + T.prefetch_ahead : -1);
         return;
     }
     grid_dep_wait();  // receivers may sit in the band rows
@@ -825,7 +828,7 @@ __global__ void __launch_bounds__(kThreads, kTileBlocks<M>) stress_kernel(const 
         if (reads_band_rows(P, k.z0)) grid_dep_wait();
         if (k.generic) edge_tile<M, false>(P, T, k.x0, k.z0, k.x_end, smem, P.src_w);
         else fast_str<M>(P, T, refs_of(maps), k.x0, k.z0, k.x_end, k.band, k.rim, smem, P.src_w,
-                         stress_tile(P, T, bid + kPrefetchAhead));
+                         T.prefetch_ahead > 0 ? stress_tile(P, T, bid + T.prefetch_ahead) : -1);
     }
 }
 

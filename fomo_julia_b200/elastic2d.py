@@ -148,18 +148,25 @@ def ricker_wavelet(f0, dt, nt: int) -> np.ndarray:
 
 
 def julia_mean(a) -> np.float32:
-    """Statistics.mean of a Float32 array as Julia computes it (pairwise sum
-    with 1024-element blocks, then one division) -- the v_ref of run.jl:57."""
+    """Statistics.mean of a Float32 array as Julia computes it -- the v_ref of
+    run.jl:57: Base's pairwise mapreduce (split at the midpoint until a block
+    holds fewer than 1024 elements), then one Float32 division by the length.
+
+    Each block is summed strictly in order here (np.cumsum accumulates in
+    Float32, one element after the other).  Julia's block loop carries
+    ``@simd``, which lets LLVM reassociate it into vector partial sums whose
+    shape depends on the host's vector width; that shape cannot be pinned
+    without Julia, so this order is exact only where the block sums are
+    (every constant-valued model, including the run.jl golden case)."""
     v = np.asfortranarray(a, dtype=f32).ravel(order="F")
+    if v.size == 0:
+        return f32(np.nan)
 
     def rec(i0: int, i1: int) -> np.float32:
         if i0 == i1:
             return v[i0]
         if i1 - i0 < 1024:
-            s = f32(v[i0] + v[i0 + 1])
-            for x in v[i0 + 2:i1 + 1]:
-                s = f32(s + x)
-            return s
+            return np.cumsum(v[i0:i1 + 1], dtype=f32)[-1]
         im = i0 + ((i1 - i0) >> 1)
         return f32(rec(i0, im) + rec(im + 1, i1))
 

@@ -245,11 +245,11 @@ int fomo_b200_shot_profile(uint64_t shot_handle, int32_t n_steps, FomoKernelTime
 int fomo_b200_selftest_wait(int32_t polls, int32_t* status);
 
 /* Allocation-free shot.  No counterpart in the reference: it exists for
- * callers that cannot allocate device memory while a shot runs -- a caller
- * capturing its stream into a CUDA graph (allocation cannot be captured), a
- * serving loop that carves all memory from a fixed pool at start-up, or a
- * host framework that forbids cudaMalloc/cudaFree (and the device-wide
- * synchronisation cudaFree implies) on its latency path.
+ * callers that cannot allocate device memory while a shot runs -- a serving
+ * loop that carves all of its memory from a fixed pool at start-up and must
+ * not fail for lack of memory later, or a host framework that forbids
+ * cudaMalloc/cudaFree (and the device-wide synchronisation cudaFree implies)
+ * on its latency path.
  *
  * Runs the same kernels as fomo_b200_run_shot and calls no cudaMalloc,
  * cudaFree or allocating library routine.  Every scratch buffer (both
@@ -267,14 +267,17 @@ int fomo_b200_selftest_wait(int32_t polls, int32_t* status);
  * aligned), the HABC and shot descriptions as for fomo_b200_run_shot (host
  * structs).  Output: gather_out, a device array of nt*n_rec floats
  * ([nt x n_rec] column major).  Work is queued on `stream` (a cudaStream_t,
- * NULL for the legacy default stream) and the call returns once it is done.
+ * NULL for the legacy default stream): the HABC tables and receiver offsets
+ * are copied from host memory with cudaMemcpyAsync, and the call waits for
+ * the stream and reads the kernels' status word back before it returns.
  * fomo_b200_init is not required; the current CUDA device is used.
  *
  * The first call on a device resolves the array's device address
- * (cudaGetSymbolAddress), so make that first call before any stream capture.
- * All calls share the array and it keeps the last call's contents; each call
- * clears what must start at zero.  Calls that overlap on the GPU race on the
- * array: serialise them. */
+ * (cudaGetSymbolAddress, with that device current) and keeps it; make that
+ * first call before any stream capture on the device.  All calls share the
+ * array and it keeps the last call's contents; each call clears what must
+ * start at zero (the wavefield and the status word).  Calls that overlap on
+ * the GPU race on the array: serialise them. */
 int fomo_b200_run_shot_noalloc(int32_t nx, int32_t nz, int32_t M, int32_t pad,
                                int32_t free_surface, const float* rho_vx,
                                const float* rho_vz, const float* lam,

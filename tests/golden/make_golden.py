@@ -6,7 +6,7 @@ It is copied verbatim; runjl_case.json records the run.jl recipe
 (run.jl:36-61, 90-131) that produced it, so the tests can rebuild the inputs
 without the reference being present.
 
-Usage:  python tests/golden/make_golden.py [/path/to/reference]
+Usage:  python tests/golden/make_golden.py /path/to/reference-checkout
 """
 import hashlib
 import json
@@ -40,4 +40,6 @@ def main(ref_root: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_golden.py /path/to/reference-checkout")
+    main(sys.argv[1])

@@ -92,6 +92,33 @@ def test_setup_receivers_and_vref():
         F.setup_receivers([1.0], [1.0, 2.0], med)
 
 
+def _mean_scalar_loop(a):
+    """Julia's pairwise Float32 sum (blocks under 1024 elements summed in
+    order, one scalar add at a time), divided by the length."""
+    f32 = np.float32
+    v = np.asfortranarray(a, dtype=f32).ravel(order="F")
+
+    def rec(i0, i1):
+        if i0 == i1:
+            return v[i0]
+        if i1 - i0 < 1024:
+            s = f32(v[i0] + v[i0 + 1])
+            for x in v[i0 + 2:i1 + 1]:
+                s = f32(s + x)
+            return s
+        im = i0 + ((i1 - i0) >> 1)
+        return f32(rec(i0, im) + rec(im + 1, i1))
+
+    return f32(rec(0, v.size - 1) / f32(v.size))
+
+
+@pytest.mark.parametrize("n", [1, 2, 3, 1023, 1024, 1025, 4099, 65537])
+def test_julia_mean_block_order(n):
+    # the vectorised block sums equal the scalar loop, block boundaries included
+    a = (np.random.default_rng(n).random(n) * 3000.0 + 1500.0).astype(np.float32)
+    assert F.julia_mean(a) == _mean_scalar_loop(a)
+
+
 def test_backend_names():
     with pytest.raises(ValueError, match="Unknown backend"):
         F.backend("cpu")

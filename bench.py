@@ -140,9 +140,10 @@ def host_inputs(w):
 
 
 # ---------------------------------------------------------------- reference arm
-def cpu_sample(w, hi, seconds: float, threads: int = 0):
+def cpu_sample(w, hi, seconds: float, threads: int = 0, keep=False):
     """Times the oracle (CPU restatement of the reference) on the first time
-    steps of the same shot; returns (Gcell-steps/s, steps, cores)."""
+    steps of the same shot; returns (Gcell-steps/s, steps, cores, seconds)
+    and, with keep, also the oracle's gather and final fields (nx, nz, 5)."""
     import oracle
     oracle.build()
     med = oracle.OMedium(hi["nx"], hi["nz"], w.fd_order // 2, hi["pad"], w.nbc, w.dx, w.dz, w.free_surface,
@@ -151,18 +152,55 @@ def cpu_sample(w, hi, seconds: float, threads: int = 0):
                                       hi["habc"].qxt], dtype=np.float32),
                      hi["habc"].w_vx, hi["habc"].w_vz, hi["habc"].w_tau)
     cells = hi["nx"] * hi["nz"]
+    out = {}
 
-    def run(n):
+    def run(n, final=False):
         t = time.perf_counter()
-        oracle.run_shot(med, h, hi["a"], w.dt, w.nt, hi["si"], hi["sj"], hi["wav"], hi["ri"], hi["rj"], "vz",
-                        "simd8", n_steps=n, n_threads=threads)
-        return time.perf_counter() - t
+        r = oracle.run_shot(med, h, hi["a"], w.dt, w.nt, hi["si"], hi["sj"], hi["wav"], hi["ri"], hi["rj"], "vz",
+                            "simd8", n_steps=n, n_threads=threads, final_fields=final)
+        dt = time.perf_counter() - t
+        if final:
+            out["gather"], out["fields"] = r
+        return dt
 
     t1 = run(2)
     n = max(2, min(w.nt, int(seconds / max(t1 / 2, 1e-6))))
-    t = run(n)
+    t = run(n, final=keep)
     cores = threads or oracle.max_threads()
+    if keep:
+        return cells * n / t / 1e9, n, cores, t, out
     return cells * n / t / 1e9, n, cores, t
+
+
+def error_stats(g, ref):
+    """Max abs error, relative L2 over the whole gather, and the largest
+    per-trace relative L2 over traces whose reference is not all zero."""
+    g = np.asarray(g, dtype=np.float64)
+    ref = np.asarray(ref, dtype=np.float64)
+    num = np.linalg.norm(g - ref, axis=0)
+    den = np.linalg.norm(ref, axis=0)
+    live = den > 0
+    return {"max_abs": float(np.abs(g - ref).max()) if g.size else 0.0,
+            "rel_l2": float(np.linalg.norm(g - ref) / max(np.linalg.norm(ref), 1e-300)),
+            "max_trace_rel_l2": float((num[live] / den[live]).max()) if live.any() else 0.0,
+            "traces_compared": int(live.sum())}
+
+
+def float64_gather(w, n):
+    """The same shot in Float64 through the oracle (init, HABC tables,
+    coefficients, wavelet and time steps all in double), first n steps."""
+    import oracle
+    import fomo_julia_b200 as F
+    med = oracle.init_medium(w.vp, w.vs, w.rho, w.dx, w.dz, w.nbc, w.fd_order, w.free_surface, dtype=np.float64)
+    h = oracle.init_habc(w.nbc, w.dt, w.dx, w.dz, float(F.julia_mean(w.vp)), dtype=np.float64)
+    a = oracle.fd_coefficients(w.fd_order, dtype=np.float64)
+    wav = oracle.ricker(w.f0, w.dt, w.nt, dtype=np.float64)
+    si = oracle.coord_to_index(w.src_x[0], w.dx, med.pad)
+    sj = oracle.coord_to_index(w.src_z[0], w.dz, med.pad)
+    ri = [oracle.coord_to_index(x, w.dx, med.pad) for x in w.rec_x]
+    rj = [oracle.coord_to_index(z, w.dz, med.pad) for z in w.rec_z]
+    return oracle.run_shot(med, h, a, w.dt, w.nt, si, sj, wav, ri, rj, "vz", "simd8", dtype=np.float64,
+                           n_steps=n)
 
 
 def reference_arm(args, rank, world):
@@ -584,12 +622,33 @@ def b200_arm(args, rank, world, local):
                     / sum(k["avg_ms"] for k in kernels),
                     "kernels": kernels}
 
-    cpu = None
+    cpu = parity = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        v, n, cores, t = cpu_sample(w, hi, args.cpu_seconds)
+        v, n, cores, t, orc = cpu_sample(w, hi, args.cpu_seconds, keep=True)
         cpu = {"value": v, "unit": METRIC, "cores": cores, "kind": "port",
                "sample": f"first {n} time steps of the same shot ({t:.1f} s), C++ restatement of the "
                          f"reference's Float32 CPU path (oracle/), OpenMP"}
+        # the same n steps on the GPU, against the oracle's answer (not timed)
+        sh = ctypes.c_uint64(0)
+        call("fomo_b200_shot_begin", med, wf, ctypes.byref(H), ctypes.byref(S), ctypes.byref(sh))
+        kd = ctypes.c_int32(0)
+        call("fomo_b200_shot_advance", sh.value, n, ctypes.byref(kd))
+        g_gpu = np.zeros((w.nt, n_rec), dtype=np.float32, order="F")
+        same_fields = True
+        for q in range(5):
+            f = np.zeros((nx, nz), dtype=np.float32, order="F")
+            call("fomo_b200_wavefield_download", wf, q, f.ctypes.data)
+            same_fields &= bool(np.array_equal(f, orc["fields"][:, :, q]))
+        call("fomo_b200_shot_finish", sh.value, g_gpu.ctypes.data, None)
+        g64 = float64_gather(w, n)
+        parity = {"steps": n, "oracle": "Float32 CPU restatement of the reference (oracle/)",
+                  "bit_exact": bool(np.array_equal(g_gpu, orc["gather"])) and same_fields,
+                  "gather_bit_exact": bool(np.array_equal(g_gpu, orc["gather"])),
+                  "final_fields_bit_exact": same_fields,
+                  **{k: v for k, v in error_stats(g_gpu, orc["gather"]).items() if k != "traces_compared"},
+                  "vs_float64": {"gpu": error_stats(g_gpu, g64), "oracle_f32": error_stats(orc["gather"], g64),
+                                 "reference": "the oracle instantiated in double (Float64 init and steps)"}}
+        del orc, g64
 
     batched = served = uneven = None
     if rank == 0 and world == 1:
@@ -621,7 +680,7 @@ def b200_arm(args, rank, world, local):
                                "note": "the same run counted on the unpadded model cells, as the reference's README counts"},
             "loop_ms_per_shot": [round(t.device_ms, 2) for t in st_v],
             "e2e": e2e, "gpu_launches": int(launches), "clocks": clocks, "roofline": roofline,
-            "cpu_baseline": cpu,
+            "cpu_baseline": cpu, "parity": parity,
             "batched": batched, "uneven": uneven, "serving": served,
         }
         print(json.dumps(line), flush=True)

@@ -108,3 +108,15 @@ def oracle_inputs(c: Case, oracle):
     ri = [oracle.coord_to_index(x, c.dx, med.pad) for x in c.rec_x]
     rj = [oracle.coord_to_index(z, c.dz, med.pad) for z in c.rec_z]
     return med, h, a, wav, si, sj, np.array(ri, np.int32), np.array(rj, np.int32)
+
+
+def case_from_workload(w, rec_type=None, shot=0, nt=None) -> Case:
+    """A parity Case for one shot of a benchmark workload
+    (fomo_julia_b200.synthetic): the same medium, time axis, source and
+    receivers, with v_ref = mean(vp) as run.jl:57 computes it."""
+    from fomo_julia_b200 import julia_mean
+    rt = rec_type or w.rec_types[0]
+    return Case(f"{w.name}_shot{shot}_{rt}" + ("" if nt is None else f"_nt{nt}"), w.vp, w.vs, w.rho,
+                float(w.dx), float(w.dz), w.nbc, w.fd_order, w.free_surface, f32(w.dt),
+                w.nt if nt is None else nt, w.f0, julia_mean(w.vp), float(w.src_x[shot]), float(w.src_z[shot]),
+                np.asarray(w.rec_x, dtype=f32), np.asarray(w.rec_z, dtype=f32), rt)

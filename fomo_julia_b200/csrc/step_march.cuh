@@ -1,0 +1,505 @@
+// step_march.cuh -- the fused time step: one launch per step computes the
+// velocity and the stress update of every cell (time_stepper.jl:39-63), so
+// each field and medium array crosses HBM once per step (read five fields and
+// five medium arrays, write five fields: 60 B per cell with dx == dz).
+//
+// Work split.  The grid is cut into column strips of W output columns (W = 56
+// for M <= 4) and each strip into row segments; one block owns one
+// (strip, segment) and marches down it in blocks of kMR = 16 rows.  At
+// iteration t it computes
+//   velocity block t   rows za - M + 16t .. +16, over the strip plus an HV-column
+//                      halo on each side (64 columns: the stress of the
+//                      strip's edge columns reads them), and
+//   stress block t-1   rows za + 16(t-1) .. +16, over the strip's own columns,
+// from velocity blocks t-1 and t, which stay in a shared-memory ring of three
+// blocks.  New velocities never go back to HBM before the stress reads them,
+// and neither the velocity halo nor the rows above a segment cost DRAM reads
+// beyond the tau boxes' overlap (served by L2).
+//
+// Data movement.  Thread 0 loads each iteration's tau box (txx, tzz, txz over
+// 72 x (16 + 2M) cells: the velocity stencil's inputs and the stress's
+// step-start values) by TMA into a four-stage ring, two iterations ahead, and
+// prefetches into L2 the boxes of the pointwise operands (vx, vz, buoyancy,
+// lam, mu, mu_xz), which the threads read with 128-bit loads.  Stage t is
+// read by velocity block t and stress block t-1, so stage t+2 is loaded into
+// the slot of stage t-2 once every thread has passed iteration t's barrier.
+//
+// Boundary rules, all inside the march:
+//   left/right HABC (boundary.jl:76-85): strips whose columns reach a band
+//     exchange their pre-HABC values through shared memory and apply the
+//     rules of step_common.cuh; the first strip holds the whole left band and
+//     the column its rule reads, the last (right-aligned) strip the whole
+//     right band and the two columns its rules read;
+//   bottom band and corners (boundary.jl:88-132): a recurrence along j; the
+//     blocks that hold band rows march them in order, one warp per 28-column
+//     strip and field, exactly as band_march does (lane rules, shuffles);
+//   free surface (boundary.jl:168-181): tzz = txz = 0 in rows pad-5..pad;
+//   source (source_receiver.jl:18-30): added to the smem copy of a tau box;
+//   receivers (source_receiver.jl:65-77): record blocks appended to the grid
+//     read the step-start copy, as in the split launches.
+// The fused step needs a free surface (no top HABC band), M <= 4 and bands
+// narrow enough for the first and last strips (march_supported); other
+// configurations run the split launches.
+#pragma once
+
+#include "step_tiled.cuh"
+
+namespace fomo {
+
+constexpr int kMR = 16;            // rows per block
+constexpr int kMVW = 64;           // velocity columns of a strip, halo included
+constexpr int kMThreads = 256;     // 16 column groups x 16 rows, one row per thread
+constexpr int kMStages = 4;        // tau box stages
+constexpr int kMRing = 3;          // velocity blocks kept
+constexpr int kMMaxSegs = 64;
+
+template <int M>
+struct MGeo {
+    static_assert(M >= 1 && M <= 4, "the fused step covers M <= 4");
+    static constexpr int HV = 4;                    // velocity halo columns (>= M, 16-byte aligned)
+    static constexpr int W = kMVW - 2 * HV;         // output columns of a strip
+    static constexpr int TW = kMVW + 2 * HV;        // tau box width
+    static constexpr int TH = kMR + 2 * M;          // tau box rows
+    static constexpr int TAU = TW * TH;             // floats of one field's box
+    static constexpr int STAGE = 3 * TAU;
+    static constexpr int RING_ROWS = kMRing * kMR;  // 48
+    static constexpr int RING = RING_ROWS * kMVW;   // floats of one field's ring
+    static constexpr int NQ = 3;                    // float4s of an x window (HV = 4)
+};
+
+// Launch-wide parameters of the fused step (besides StepParams).
+struct MarchArgs {
+    const float* b[4];     // buoyancy dtx/rho_vx, dtz/rho_vx, dtx/rho_vz, dtz/rho_vz
+    int iso;
+    int* status;
+    int n_strips, n_segs, n_items;
+    int x_last;            // first output column of the last (right-aligned) strip
+    int seg_z[kMMaxSegs + 1];  // segment s: stress rows [seg_z[s], seg_z[s+1])
+};
+
+// Descriptors: tau boxes (TW x TH) of the step-start copy; L2-prefetch boxes
+// (64 x 16) of the pointwise operands.
+struct MarchMaps {
+    CUtensorMap xx, zz, xz;        // halo boxes of txx, tzz, txz (copy a)
+    CUtensorMap vx, vz;            // tile boxes of vx, vz (copy a)
+    CUtensorMap b0, b1, b2, b3;    // tile boxes of the buoyancy arrays
+    CUtensorMap lam, mu, mxz;      // tile boxes of the medium
+};
+
+template <int M>
+__host__ __device__ constexpr size_t march_smem_floats() {
+    using G = MGeo<M>;
+    return (size_t)kMStages * G::STAGE + 2 * (size_t)G::RING + 3 * kMVW;
+}
+template <int M>
+__host__ constexpr size_t march_smem_bytes() {
+    return march_smem_floats<M>() * 4 + kMStages * 8 + 16;
+}
+
+__device__ __forceinline__ bool mbar_wait_parity(uint64_t* bar, uint32_t parity, int* status) {
+    for (int it = 0; it < kWaitPolls; ++it)
+        if (mbar_try_wait(bar, parity)) return true;
+    atomicCAS(status, 0, kErrTmaTimeout);
+    return false;
+}
+
+__device__ __forceinline__ void fence_proxy_async_smem() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+// d = sum_l a_l (w[M+l-1] - w[M-l]) over a 2M-row window (one row per thread),
+// in the reference's accumulation order.
+template <int M>
+__device__ __forceinline__ float4 zderiv1(const StepParams& P, const float4 (&w)[2 * M]) {
+    float4 d = make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+    for (int l = 1; l <= M; ++l) {
+        const float al = P.a[l - 1];
+        d.x = fadd(fmul(al, fsub(w[M + l - 1].x, w[M - l].x)), d.x);
+        d.y = fadd(fmul(al, fsub(w[M + l - 1].y, w[M - l].y)), d.y);
+        d.z = fadd(fmul(al, fsub(w[M + l - 1].z, w[M - l].z)), d.z);
+        d.w = fadd(fmul(al, fsub(w[M + l - 1].w, w[M - l].w)), d.w);
+    }
+    return d;
+}
+
+// x-derivative of 4 columns from a 12-wide window starting HV = 4 cells left
+// of the first column; S = 0: f[i+l-1] - f[i-l], S = 1: f[i+l] - f[i-l+1].
+template <int M, int S>
+__device__ __forceinline__ float4 xderiv1(const StepParams& P, const float* row) {
+    float w[12];
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+        const float4 v = lds4(row + 4 * q);
+        w[4 * q] = v.x;
+        w[4 * q + 1] = v.y;
+        w[4 * q + 2] = v.z;
+        w[4 * q + 3] = v.w;
+    }
+    float d[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+        float acc = 0.f;
+#pragma unroll
+        for (int l = 1; l <= M; ++l) acc = fadd(fmul(P.a[l - 1], fsub(w[4 + c + l - 1 + S], w[4 + c - l + S])), acc);
+        d[c] = acc;
+    }
+    return make_float4(d[0], d[1], d[2], d[3]);
+}
+
+__device__ __forceinline__ float4 add4(float4 a, float4 b) {
+    return make_float4(fadd(a.x, b.x), fadd(a.y, b.y), fadd(a.z, b.z), fadd(a.w, b.w));
+}
+__device__ __forceinline__ float4 mul4(float4 a, float4 b) {
+    return make_float4(fmul(a.x, b.x), fmul(a.y, b.y), fmul(a.z, b.z), fmul(a.w, b.w));
+}
+__device__ __forceinline__ float4 mul4s(float4 a, float s) {
+    return make_float4(fmul(a.x, s), fmul(a.y, s), fmul(a.z, s), fmul(a.w, s));
+}
+
+// Values of one field over a shared-memory row-major region whose row r0
+// holds grid row z0 and column 0 grid column xs (rows wrap after `rows`).
+struct SmemRows {
+    const float* base;
+    int xs, z0, r0, rows, pitch;
+    __device__ float operator()(int i, int j) const {
+        int r = r0 + (j - z0);
+        r = r >= rows ? r - rows : (r < 0 ? r + rows : r);
+        return base[r * pitch + (i - xs)];
+    }
+};
+
+// The bottom-band recurrence (rows nz-nbc-1 .. nz-2) of one field over the
+// band rows [ja, jb) of one block: `pre` holds the block's values after the
+// stencil update (band rows) and final values (rows above), and receives the
+// finals in place.  One warp per 28-column strip: lane l holds column
+// xs - 2 + l; lanes 2..29 write back and store (own columns only).  The lane
+// rules are band_march's.
+// `prev` (column 0 = pre_xs), when given, holds the finals of row ja - 1;
+// otherwise that row is read from `pre`.
+__device__ __forceinline__ void march_band_rows(const StepParams& P, const float* tab, const float* oin, float* oout,
+                                                float* pre, int pre_pitch, int pre_xs, int pre_z0, int pre_r0,
+                                                int pre_rows, int c_lo, int c_hi, int own_lo, int own_hi, int xs,
+                                                int ja, int jb, const float* prev) {
+    constexpr unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const int b = P.nbc, nx = P.nx, nz = P.nz, r0 = nx - b - 1;
+    const int i = xs - 2 + lane;
+    const bool have = i >= c_lo && i < c_hi && i >= 0 && i < nx;  // the lane's column holds a value
+    const bool rim = i <= 0 || i >= nx - 1;
+    const bool left = i >= 1 && i <= b;
+    const bool corner = left || (i >= r0 && i <= nx - 2);
+    const bool redo = i == b || (i > r0 - 1 && i <= nx - 2 && right_chunk_start(nx, b, i));
+    const int nb = min(max(lane + (left ? 1 : -1), 0), 31);
+    const int dxi = max(min(i, nx - 1 - i), 0);
+    auto at = [&](int j) -> float* {
+        int r = pre_r0 + (j - pre_z0);
+        r = r >= pre_rows ? r - pre_rows : (r < 0 ? r + pre_rows : r);
+        return pre + r * pre_pitch + (i - pre_xs);
+    };
+    float fprev = have ? (prev ? prev[i - pre_xs] : *at(ja - 1)) : 0.f;
+    float ovp = have ? __ldg(oin + cell(P, i, ja - 1)) : 0.f;
+    const bool store = have && lane >= 2 && lane < 30;
+    const bool own = store && i >= own_lo && i < own_hi;
+    for (int j = ja; j < jb; ++j) {
+        const float pv = have ? *at(j) : 0.f;
+        const float ov = have ? __ldg(oin + cell(P, i, j)) : 0.f;
+        const float w = __ldg(tab + min(min(dxi, nz - 1 - j), b + 1));
+        const float pv_nb = __shfl_sync(FULL, pv, nb);
+        const float ov_nb = __shfl_sync(FULL, ov, nb);
+        const float sz = edge_sum(P.qz, P.qt_z, P.qxt, fprev, ov, ovp);
+        const float fc = blend_corner(w, pv, edge_sum(P.qx, P.qt_x, P.qxt, pv_nb, ov, ov_nb), sz);
+        const float fe = blend_edge(w, pv, sz);
+        const float fa = rim ? pv : (corner ? fc : fe);
+        const float fa_nb = __shfl_sync(FULL, fa, nb);
+        const float fb = blend_corner(w, pv, edge_sum(P.qx, P.qt_x, P.qxt, fa_nb, ov, ov_nb), sz);
+        const float fin = redo ? fb : fa;
+        if (store) *at(j) = fin;
+        if (own) oout[cell(P, i, j)] = fin;
+        fprev = fin;
+        ovp = ov;
+    }
+}
+
+template <int M>
+__global__ void __launch_bounds__(kMThreads, 2)
+    march_kernel(const __grid_constant__ StepParams P, const __grid_constant__ MarchArgs A,
+                 const __grid_constant__ MarchMaps mp) {
+    using G = MGeo<M>;
+    extern __shared__ __align__(128) float smem[];
+    const int bid = blockIdx.x;
+    if (bid >= A.n_items) {
+        record_block(P, bid - A.n_items, P.rec_k);
+        return;
+    }
+    // Items: bottom segments first (they march the band), and within a
+    // segment the two edge strips first (they apply the side rules).
+    const int seg = A.n_segs - 1 - bid / A.n_strips;
+    const int k = bid % A.n_strips;
+    const int strip = k == 0 ? 0 : (k == 1 ? A.n_strips - 1 : k - 1);
+    const bool last_strip = strip == A.n_strips - 1;
+    const int x0 = last_strip ? A.x_last : strip * G::W;
+    const int x_end = last_strip ? min(x0 + G::W, (P.nx + 3) / 4 * 4) : min(x0 + G::W, A.x_last);
+    const int xa = x0 - G::HV;
+    const int za = A.seg_z[seg], zb = A.seg_z[seg + 1];
+    const int n_it = (zb - za + kMR - 1) / kMR + 1;  // velocity blocks 0..n_it-1; stress blocks 0..n_it-2
+    const int nx = P.nx, nz = P.nz, b = P.nbc;
+    const int j0 = nz - b - 1;                        // first bottom-band row
+    const int edge = max(b + 2, M);
+    const bool side = xa < edge || xa + kMVW > nx - edge;  // block-uniform: side HABC or rim columns
+
+    float* stage = smem;
+    float* ring = smem + kMStages * G::STAGE;          // [2 fields][48 rows][64]
+    float* s_last = ring + 2 * G::RING;                // [3][64] stress finals of the last row of a block
+    uint64_t* full = reinterpret_cast<uint64_t*>(s_last + 3 * kMVW);
+
+    auto issue = [&](int t) {
+        const int s = t % kMStages;
+        float* dst = stage + s * G::STAGE;
+        const int vr0 = za - M + t * kMR;
+        mbar_expect_tx(full + s, 3 * G::TAU * 4);
+        tma_load_2d(dst, &mp.xx, x0 - 2 * G::HV, vr0 - M, full + s);
+        tma_load_2d(dst + G::TAU, &mp.zz, x0 - 2 * G::HV, vr0 - M, full + s);
+        tma_load_2d(dst + 2 * G::TAU, &mp.xz, x0 - 2 * G::HV, vr0 - M, full + s);
+        tma_prefetch_2d(&mp.vx, xa, vr0);
+        tma_prefetch_2d(&mp.vz, xa, vr0);
+        tma_prefetch_2d(&mp.b0, xa, vr0);
+        tma_prefetch_2d(&mp.b2, xa, vr0);
+        if (!A.iso) {
+            tma_prefetch_2d(&mp.b1, xa, vr0);
+            tma_prefetch_2d(&mp.b3, xa, vr0);
+        }
+        tma_prefetch_2d(&mp.lam, x0, vr0 + M);
+        tma_prefetch_2d(&mp.mu, x0, vr0 + M);
+        tma_prefetch_2d(&mp.mxz, x0, vr0 + M);
+    };
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < kMStages; ++s) mbar_init(full + s, 1);
+        fence_barrier_init();
+        for (int t = 0; t < min(kMStages, n_it); ++t) issue(t);
+    }
+    __syncthreads();
+
+    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+    const int xv = xa + 4 * tx;          // first column of the thread's velocity cells
+    const int xs = x0 + 4 * tx;          // first column of the thread's stress cells (tx < W/4)
+    const bool s_col = tx < G::W / 4;
+    const bool v_own = xv >= x0 && xv < x_end;
+    const bool s_own = s_col && xs < x_end;
+    const bool v_in = xv >= 0 && xv < nx;
+    const bool s_in = s_col && xs < nx;
+    const int warp = threadIdx.x >> 5;
+
+    for (int t = 0; t < n_it; ++t) {
+        const int s = t % kMStages;
+        float* tau = stage + s * G::STAGE;
+        if (!mbar_wait_parity(full + s, (t / kMStages) & 1, A.status)) return;
+        // ------------------------------------------------ the source, into this stage's copy
+        const int vr0 = za - M + t * kMR;
+        {
+            const int si = P.src_i - (x0 - 2 * G::HV), sj = P.src_j - (vr0 - M);
+            if (si >= 0 && si < G::TW && sj >= 0 && sj < G::TH) {  // block-uniform
+                if (threadIdx.x == 0) {
+                    tau[sj * G::TW + si] = fadd(tau[sj * G::TW + si], P.src_w);
+                    tau[G::TAU + sj * G::TW + si] = fadd(tau[G::TAU + sj * G::TW + si], P.src_w);
+                }
+                __syncthreads();
+            }
+        }
+        // ------------------------------------------------ velocity block t
+        {
+            const int j = vr0 + ty;
+            // rows the stress of this segment reads: the last block feeds 2M stress rows
+            const int v_hi = min(vr0 + (t < n_it - 1 ? kMR : 2 * M), zb + M);
+            float4 ox = make_float4(0.f, 0.f, 0.f, 0.f), oz = ox;
+            const bool row_ok = j < v_hi && j >= 0 && j < nz;
+            if (row_ok && v_in) {
+                const size_t c = cell(P, xv, j);
+                const float4 vx = ldg4(P.in[VX] + c), vz = ldg4(P.in[VZ] + c);
+                const float4 b0 = ldg4(A.b[0] + c), b2 = ldg4(A.b[2] + c);
+                const float4 b1 = A.iso ? b0 : ldg4(A.b[1] + c), b3 = A.iso ? b2 : ldg4(A.b[3] + c);
+                const float* rxx = tau + (ty + M) * G::TW + 4 * tx;             // window from column xv - 4
+                const float* rxz = tau + 2 * G::TAU + (ty + M) * G::TW + 4 * tx;
+                const float4 d1 = xderiv1<M, 0>(P, rxx);   // dtxx/dx: txx[i+l-1] - txx[i-l]
+                const float4 d3 = xderiv1<M, 1>(P, rxz);   // dtxz/dx: txz[i+l] - txz[i-l+1]
+                float4 wz[2 * M];
+#pragma unroll
+                for (int q = 0; q < 2 * M; ++q) wz[q] = lds4(tau + 2 * G::TAU + (ty + q) * G::TW + 4 * tx + G::HV);
+                const float4 d2 = zderiv1<M>(P, wz);        // dtxz/dz: txz[j+l-1] - txz[j-l]
+#pragma unroll
+                for (int q = 0; q < 2 * M; ++q) wz[q] = lds4(tau + G::TAU + (ty + 1 + q) * G::TW + 4 * tx + G::HV);
+                const float4 d4 = zderiv1<M>(P, wz);        // dtzz/dz: tzz[j+l] - tzz[j-l+1]
+                ox = add4(vx, add4(mul4(b0, d1), mul4(b1, d2)));
+                oz = add4(vz, add4(mul4(b2, d3), mul4(b3, d4)));
+                if (side || j < M || j > nz - 1 - M) {
+#pragma unroll
+                    for (int c4 = 0; c4 < 4; ++c4)
+                        if (!in_stencil(P, xv + c4, j)) {
+                            set_comp(ox, c4, comp(vx, c4));
+                            set_comp(oz, c4, comp(vz, c4));
+                        }
+                }
+            }
+            const int rr = (t % kMRing) * kMR + ty;    // ring row of grid row j
+            float* rvx = ring + rr * kMVW + 4 * tx;
+            float* rvz = ring + G::RING + rr * kMVW + 4 * tx;
+            *reinterpret_cast<float4*>(rvx) = ox;
+            *reinterpret_cast<float4*>(rvz) = oz;
+            const bool band_rows = v_hi > j0 && vr0 <= nz - 2;  // block-uniform
+            if (side || band_rows) {
+                __syncthreads();  // pre values of the block in the ring
+                if (side && row_ok && j >= b && j <= j0 - 1) {  // left/right HABC (free surface: rows nbc .. nz-nbc-2)
+                    const SmemRows pvx{ring, xa, vr0, (t % kMRing) * kMR, G::RING_ROWS, kMVW};
+                    const SmemRows pvz{ring + G::RING, xa, vr0, (t % kMRing) * kMR, G::RING_ROWS, kMVW};
+                    const HabcPoint<SmemRows> hx{P, pvx, P.in[VX], P.w_tab[0]};
+                    const HabcPoint<SmemRows> hz{P, pvz, P.in[VZ], P.w_tab[1]};
+#pragma unroll
+                    for (int c4 = 0; c4 < 4; ++c4) {
+                        const int i = xv + c4;
+                        // the rule's neighbours must lie in the strip's columns
+                        if (i > xa && i < xa + kMVW - 1 && lr_band_cell(P, i, j) &&
+                            (i <= b || i - 2 >= xa)) {
+                            set_comp(ox, c4, hx.final_value(i, j));
+                            set_comp(oz, c4, hz.final_value(i, j));
+                        }
+                    }
+                }
+                __syncthreads();
+                *reinterpret_cast<float4*>(rvx) = ox;
+                *reinterpret_cast<float4*>(rvz) = oz;
+                if (band_rows) {
+                    __syncthreads();
+                    if (warp < 6) {
+                        const int f = warp / 3, ws = warp % 3;
+                        march_band_rows(P, P.w_tab[f], P.in[VX + f], P.out[VX + f], ring + f * G::RING, kMVW, xa,
+                                        vr0, (t % kMRing) * kMR, G::RING_ROWS, xa, xa + kMVW, x0, x_end,
+                                        xa + 28 * ws, max(vr0, j0), min(v_hi, nz - 1), nullptr);
+                    }
+                    __syncthreads();
+                    ox = *reinterpret_cast<const float4*>(rvx);
+                    oz = *reinterpret_cast<const float4*>(rvz);
+                }
+            }
+            if (row_ok && v_own && !(j >= j0 && j <= nz - 2)) {  // band rows were stored by the march
+                stg4(P.out[VX] + cell(P, xv, j), ox);
+                stg4(P.out[VZ] + cell(P, xv, j), oz);
+            }
+        }
+        __syncthreads();  // velocity block t in the ring; every thread is done with iteration t-1
+        if (threadIdx.x == 0 && t >= 2 && t + 2 < n_it) {
+            fence_proxy_async_smem();  // generic accesses of the slot before the TMA overwrites it
+            issue(t + 2);
+        }
+        // ------------------------------------------------ stress block t-1
+        if (t >= 1) {
+            const int sr0 = za + (t - 1) * kMR;
+            const int j = sr0 + ty;
+            const float* told = stage + ((t - 1) % kMStages) * G::STAGE;  // stage t-1: rows from sr0 - 2M
+            const bool row_ok = j < zb && j < nz;
+            float4 oxx = make_float4(0.f, 0.f, 0.f, 0.f), ozz = oxx, oxz = oxx;
+            if (row_ok && s_in) {
+                const size_t c = cell(P, xs, j);
+                const float4 lam = ldg4(P.lam + c), mu = ldg4(P.mu_txx + c), mxz = ldg4(P.mu_txz + c);
+                const int bo = (ty + 2 * M) * G::TW + 2 * G::HV + 4 * tx;
+                const float4 txx = lds4(told + bo), tzz = lds4(told + G::TAU + bo), txz = lds4(told + 2 * G::TAU + bo);
+                // ring row of grid row j - M (relative row (t-1)*16 + ty)
+                int r = (((t - 1) % kMRing) * kMR + ty);
+                const float* rvx = ring + 4 * tx;
+                const float* rvz = ring + G::RING + 4 * tx;
+                const float4 dxx = xderiv1<M, 1>(P, rvx + (r + M) % G::RING_ROWS * kMVW);  // vx[i+l] - vx[i-l+1]
+                const float4 dzx = xderiv1<M, 0>(P, rvz + (r + M) % G::RING_ROWS * kMVW);  // vz[i+l-1] - vz[i-l]
+                float4 wz[2 * M];
+#pragma unroll
+                for (int q = 0; q < 2 * M; ++q) wz[q] = lds4(rvz + (r + q) % G::RING_ROWS * kMVW + G::HV);
+                const float4 dzz = zderiv1<M>(P, wz);       // vz[j+l-1] - vz[j-l]
+#pragma unroll
+                for (int q = 0; q < 2 * M; ++q) wz[q] = lds4(rvx + (r + 1 + q) % G::RING_ROWS * kMVW + G::HV);
+                const float4 dxz = zderiv1<M>(P, wz);       // vx[j+l] - vx[j-l+1]
+                const float4 l2m = add4(lam, mul4s(mu, 2.f));
+                const float4 ex = mul4s(dxx, P.dtx), ez = mul4s(dzz, P.dtz);
+                oxx = add4(txx, add4(mul4(l2m, ex), mul4(lam, ez)));
+                ozz = add4(tzz, add4(mul4(lam, ex), mul4(l2m, ez)));
+                oxz = add4(txz, mul4(mxz, add4(mul4s(dxz, P.dtz), mul4s(dzx, P.dtx))));
+                if (side || j < M || j > nz - 1 - M) {
+#pragma unroll
+                    for (int c4 = 0; c4 < 4; ++c4)
+                        if (!in_stencil(P, xs + c4, j)) {
+                            set_comp(oxx, c4, comp(txx, c4));
+                            set_comp(ozz, c4, comp(tzz, c4));
+                            set_comp(oxz, c4, comp(txz, c4));
+                        }
+                }
+            }
+            const bool band_rows = sr0 + kMR > j0 && sr0 <= nz - 2 && sr0 < zb;  // block-uniform
+            if (side || band_rows) {
+                // exchange through the slot of stage t-1 once every thread has read it
+                __syncthreads();
+                float* sp = stage + ((t - 1) % kMStages) * G::STAGE;  // [3][16][64], column 0 = x0
+                if (s_col) {
+                    *reinterpret_cast<float4*>(sp + ty * kMVW + 4 * tx) = oxx;
+                    *reinterpret_cast<float4*>(sp + kMR * kMVW + ty * kMVW + 4 * tx) = ozz;
+                    *reinterpret_cast<float4*>(sp + 2 * kMR * kMVW + ty * kMVW + 4 * tx) = oxz;
+                }
+                __syncthreads();
+                if (side && row_ok && s_in && j >= b && j <= j0 - 1) {
+                    const SmemRows p0{sp, x0, sr0, 0, kMR, kMVW};
+                    const SmemRows p1{sp + kMR * kMVW, x0, sr0, 0, kMR, kMVW};
+                    const SmemRows p2{sp + 2 * kMR * kMVW, x0, sr0, 0, kMR, kMVW};
+                    const HabcPoint<SmemRows> h0{P, p0, P.in[TXX], P.w_tab[2]};
+                    const HabcPoint<SmemRows> h1{P, p1, P.in[TZZ], P.w_tab[2]};
+                    const HabcPoint<SmemRows> h2{P, p2, P.in[TXZ], P.w_tab[2]};
+#pragma unroll
+                    for (int c4 = 0; c4 < 4; ++c4) {
+                        const int i = xs + c4;
+                        if (i >= x0 && i < x0 + G::W - 1 && lr_band_cell(P, i, j) && (i <= b || i - 2 >= x0)) {
+                            set_comp(oxx, c4, h0.final_value(i, j));
+                            set_comp(ozz, c4, h1.final_value(i, j));
+                            set_comp(oxz, c4, h2.final_value(i, j));
+                        }
+                    }
+                }
+                __syncthreads();
+                if (s_col) {
+                    *reinterpret_cast<float4*>(sp + ty * kMVW + 4 * tx) = oxx;
+                    *reinterpret_cast<float4*>(sp + kMR * kMVW + ty * kMVW + 4 * tx) = ozz;
+                    *reinterpret_cast<float4*>(sp + 2 * kMR * kMVW + ty * kMVW + 4 * tx) = oxz;
+                }
+                if (band_rows) {
+                    const int ja = max(sr0, j0), jb = min(min(sr0 + kMR, nz - 1), zb);
+                    __syncthreads();
+                    if (warp < 6) {
+                        const int f = warp / 2, ws = warp % 2;
+                        // the row above the first band row: in this block, or the previous block's last row
+                        march_band_rows(P, P.w_tab[2], P.in[TXX + f], P.out[TXX + f], sp + f * kMR * kMVW, kMVW, x0,
+                                        sr0, 0, kMR, x0, x0 + G::W, x0, x_end, x0 + 28 * ws, ja, jb,
+                                        ja == sr0 ? s_last + f * kMVW : nullptr);
+                    }
+                    __syncthreads();
+                    if (s_col) {
+                        oxx = *reinterpret_cast<const float4*>(sp + ty * kMVW + 4 * tx);
+                        ozz = *reinterpret_cast<const float4*>(sp + kMR * kMVW + ty * kMVW + 4 * tx);
+                        oxz = *reinterpret_cast<const float4*>(sp + 2 * kMR * kMVW + ty * kMVW + 4 * tx);
+                    }
+                }
+            }
+            if (row_ok && s_own) {
+                if (in_free_surface_rows(P, j)) {
+                    ozz = make_float4(0.f, 0.f, 0.f, 0.f);
+                    oxz = ozz;
+                }
+                if (!(j >= j0 && j <= nz - 2)) {
+                    stg4(P.out[TXX] + cell(P, xs, j), oxx);
+                    stg4(P.out[TZZ] + cell(P, xs, j), ozz);
+                    stg4(P.out[TXZ] + cell(P, xs, j), oxz);
+                }
+            }
+            if (ty == kMR - 1 && s_col) {  // the block's last row, read by the next block's band march
+                *reinterpret_cast<float4*>(s_last + 4 * tx) = oxx;
+                *reinterpret_cast<float4*>(s_last + kMVW + 4 * tx) = ozz;
+                *reinterpret_cast<float4*>(s_last + 2 * kMVW + 4 * tx) = oxz;
+            }
+        }
+    }
+}
+
+}  // namespace fomo

@@ -52,6 +52,9 @@ def parse():
     p.add_argument("--batch-nt", type=int, default=None, help="override nt of the batched section (development)")
     p.add_argument("--serve-requests", type=int, default=48)
     p.add_argument("--no-uneven", action="store_true", help="skip the uneven-batch section")
+    p.add_argument("--step-kernel", choices=["auto", "split", "fused"], default="auto",
+                   help="single-shot time-step kernels: the fused step where it applies (auto), or one of the two")
+    p.add_argument("--segs", type=int, default=0, help="fused step: row segments per column strip (0 = auto)")
     return p.parse_args()
 
 
@@ -472,6 +475,7 @@ def b200_arm(args, rank, world, local):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
                                 device_id=torch.device("cuda", local))
     _lib.ensure_init(local)
+    F.set_step_kernel(args.step_kernel, args.segs)
     sp = ctypes.c_void_p(0)
     call("fomo_b200_get_stream", ctypes.byref(sp))
     stream = torch.cuda.ExternalStream(sp.value, device=torch.device("cuda", local))
@@ -588,7 +592,7 @@ def b200_arm(args, rank, world, local):
     call("fomo_b200_shot_begin", med, wf, ctypes.byref(H), ctypes.byref(S), ctypes.byref(sh))
     kt = (FomoKernelTime * 8)()
     nk = ctypes.c_int32(0)
-    call("fomo_b200_shot_profile", sh.value, min(args.profile_steps, w.nt), kt, 8, ctypes.byref(nk))
+    call("fomo_b200_shot_profile", sh.value, min(args.profile_steps, w.nt), kt, 5, ctypes.byref(nk))
     call("fomo_b200_shot_finish", sh.value, None, None)
     kernels = []
     for i in range(nk.value):
@@ -675,6 +679,7 @@ def b200_arm(args, rank, world, local):
             "config": {"workload": w.name, "cells_padded": cells, "grid_padded": [nx, nz], "nt": w.nt,
                        "shots_per_gpu_per_step": 1, "parallelism": f"shot-sharded x{world}",
                        "l2": "inputs larger than L2 (357 MB medium + 715 MB state per shot)",
+                       "step_kernel": args.step_kernel,
                        "bytes_per_cell_step_algorithmic": 60},
             "physical_cells": {"cells": w.nx_in * w.nz_in,
                                "value": value * (w.nx_in * w.nz_in) / cells,

@@ -5,7 +5,7 @@ The compute lives in ``libfomo_b200.so`` (C ABI: ``include/fomo_b200.h``);
 this package is the host-side mirror of the reference's API for that path.
 """
 from .elastic2d import (  # noqa: F401
-    AbstractBackend, B200Backend, B200_BACKEND, backend, to_device, synchronize,
+    AbstractBackend, B200Backend, B200_BACKEND, backend, to_device, synchronize, set_step_kernel,
     DeviceArray, Medium, HABCConfig, Wavefield, Source, Receivers, SimParams, sim_params,
     TimeStepInfo, ShotResult, ShotConfig, MultiShotConfig, multi_shot_config,
     get_fd_coefficients, ricker_wavelet, julia_mean, init_medium, init_medium_device, init_habc, setup_receivers,

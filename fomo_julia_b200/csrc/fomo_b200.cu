@@ -22,6 +22,8 @@
 
 #include "../../include/fomo_b200.h"
 #include "step_tiled.cuh"
+#include "march_launch.h"
+#include "step_march.cuh"
 
 namespace {
 
@@ -376,7 +378,7 @@ void fill_common(fomo::StepParams& P, const Medium& m, const Shot& s) {
 // Per-launch event pairs, filled only by fomo_b200_shot_profile.
 struct Profile {
     std::vector<cudaEvent_t> ev;      // 2 per launch
-    std::vector<int> kind;            // 0 velocity, 1 stress, 2 band (velocity), 3 band (stress)
+    std::vector<int> kind;            // 0 velocity, 1 stress, 2 band (velocity), 3 band (stress), 4 fused step
     int add(cudaStream_t st, int k) {
         cudaEvent_t a, b;
         if (cudaEventCreate(&a) != cudaSuccess || cudaEventCreate(&b) != cudaSuccess) return -1;
@@ -420,8 +422,197 @@ static cudaError_t launch_tiles(void (*kern)(Exp...), int blocks, size_t smem, c
     return cudaLaunchKernelEx(&cfg, kern, std::forward<Act>(args)...);
 }
 
+// ---------------------------------------------------------------- fused step
+std::atomic<int> g_step_mode{FOMO_STEP_AUTO};
+std::atomic<int> g_march_segs{0};
+
+// Strips, segments and the validity check of one fused-step layout.
+struct MarchPlan {
+    bool ok = false;
+    char why[160] = {0};
+    fomo::MarchArgs A;
+};
+
+// Fused-step layout of an (nx, nz) grid, or the reason there is none.
+// Every boundary rule a strip needs must read only columns the strip
+// computes: the left HABC rule of cell i reads i+1, the right rule i-1 and
+// (at chunk starts) i-2, for the velocity columns the strip's stress reads
+// (own columns +- M, computed over own columns +- HV) and for its own stress
+// columns; the corners of the bottom band read the same neighbours.
+template <int M>
+MarchPlan march_plan(int nx, int nz, int nbc, bool fs, int slots, int segs_req) {
+    using G = fomo::MGeo<M>;
+    MarchPlan p;
+    std::memset(&p.A, 0, sizeof(p.A));
+#define FOMO_NO(...) (std::snprintf(p.why, sizeof(p.why), __VA_ARGS__), p)
+    if (!fs) return FOMO_NO("no free surface (the fused step has no top HABC band)");
+    const int W = G::W, HV = G::HV, VW = fomo::kMVW;
+    const int x_last = std::max(0, (nx + 3) / 4 * 4 - W);
+    const int S = x_last > 0 ? (x_last + W - 1) / W + 1 : 1;
+    const int r0 = nx - nbc - 1, j0 = nz - nbc - 1;
+    for (int st = 0; st < S; ++st) {
+        const bool last = st == S - 1;
+        const int x0 = last ? x_last : st * W;
+        const int x_end = last ? std::min(x0 + W, (nx + 3) / 4 * 4) : std::min(x0 + W, x_last);
+        const int xa = x0 - HV;
+        for (int i = std::max(0, x0 - M); i < std::min(nx, x_end + M); ++i) {
+            if (i >= 1 && i <= nbc && !(i + 1 < xa + VW))
+                return FOMO_NO("left HABC column %d needs column %d beyond strip %d", i, i + 1, st);
+            if (i >= r0 && i <= nx - 2 && !(i - 2 >= xa))
+                return FOMO_NO("right HABC column %d needs column %d before strip %d", i, i - 2, st);
+        }
+        for (int i = x0; i < std::min(nx, x_end); ++i) {
+            if (i >= 1 && i <= nbc && !(i + 1 < x0 + W))
+                return FOMO_NO("left HABC column %d needs stress column %d beyond strip %d", i, i + 1, st);
+            if (i >= r0 && i <= nx - 2 && !(i - 2 >= x0))
+                return FOMO_NO("right HABC column %d needs stress column %d before strip %d", i, i - 2, st);
+        }
+    }
+    // Row segments: the last one holds the bottom band, the row above it and
+    // the M rows its velocity reads above that.
+    const int last_max = j0 - M;
+    if (last_max < 0) return FOMO_NO("grid too shallow for the fused step");
+#undef FOMO_NO
+    int ns = segs_req;
+    if (ns <= 0) {  // fewest whole waves x rows per segment (plus ~1.5 blocks of pipeline fill)
+        long best = -1;
+        for (int c = 1; c <= std::min(fomo::kMMaxSegs, std::max(1, nz / 32)); ++c) {
+            const long waves = ((long)S * c + slots - 1) / slots;
+            const long cost = waves * ((nz + c - 1) / c + 24);
+            if (best < 0 || cost < best) {
+                best = cost;
+                ns = c;
+            }
+        }
+    }
+    ns = std::max(1, std::min(ns, fomo::kMMaxSegs));
+    for (;; --ns) {
+        const int h = (nz + ns - 1) / ns;
+        bool okz = true;
+        for (int q = 0; q < ns; ++q) p.A.seg_z[q] = q * h;
+        p.A.seg_z[ns] = nz;
+        if (ns > 1) p.A.seg_z[ns - 1] = std::min(p.A.seg_z[ns - 1], last_max);
+        for (int q = 0; q < ns; ++q) okz = okz && p.A.seg_z[q + 1] > p.A.seg_z[q];
+        if (okz || ns == 1) break;
+    }
+    p.A.n_strips = S;
+    p.A.n_segs = ns;
+    p.A.n_items = S * ns;
+    p.A.x_last = x_last;
+    p.ok = true;
+    return p;
+}
+
+// Fused-step blocks resident on the device at once (two per SM if the
+// occupancy query fails).
+template <int M>
+int march_slots() {
+    static int slots[64] = {0};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
+        (void)cudaGetLastError();
+        return 2 * sm_count();
+    }
+    if (!slots[dev]) {
+        int per_sm = 0;
+        if (raise_smem_limit(fomo::march_kernel_fn<M>(), fomo::march_smem_bytes<M>()) != FOMO_OK ||
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fomo::march_kernel_fn<M>(), fomo::kMThreads,
+                                                          fomo::march_smem_bytes<M>()) != cudaSuccess) {
+            (void)cudaGetLastError();
+            per_sm = 2;
+        }
+        slots[dev] = std::max(1, per_sm) * sm_count();
+    }
+    return slots[dev];
+}
+
+template <int M>
+int run_steps_march(Shot& s, Medium& m, Wavefield& w, int n_steps, Profile* prof, const MarchPlan& plan) {
+    static_assert(fomo::Geo<M>::BOXW == fomo::MGeo<M>::TW && fomo::Geo<M>::BOXH == fomo::MGeo<M>::TH,
+                  "the wavefield's halo descriptors are the fused step's tau boxes");
+    auto& C = ctx();
+    const bool iso = s.dtx == s.dtz;
+    if (int rc = raise_smem_limit(fomo::march_kernel_fn<M>(), fomo::march_smem_bytes<M>())) return rc;
+    if (w.map_M != M)
+        if (int rc = make_maps<M>(w)) return rc;
+    if (int rc = ensure_buoyancy(m, s.dtx, s.dtz)) return rc;
+    if (int rc = make_medium_maps(m)) return rc;
+    fomo::MarchArgs A = plan.A;
+    buoyancy_ptrs(m, A.b);
+    A.iso = iso ? 1 : 0;
+    A.status = C.d_status;
+    const int rec_blocks = (s.n_rec + fomo::kMThreads - 1) / fomo::kMThreads;
+    CUDA_TRY(cudaEventRecord(C.ev0, C.stream));
+    const int k_begin = s.k_done + 1, k_end = std::min(s.nt, s.k_done + n_steps);
+    nvtxRangePushA("fomo_b200 time loop (fused step)");
+    for (int k = k_begin; k <= k_end; ++k) {
+        const int a = w.cur, b = 1 - w.cur;
+        fomo::StepParams P;
+        fill_common(P, m, s);
+        P.src_w = (k <= (int)s.wavelet.size()) ? s.wavelet[k - 1] : 0.f;
+        for (int q = 0; q < 5; ++q) {
+            P.in[q] = w.field(a, q);
+            P.out[q] = w.field(b, q);
+        }
+        P.rec_k = (k >= 2 && s.n_rec > 0) ? k - 1 : 0;
+        fomo::MarchMaps mp;
+        mp.xx = w.maps[a][fomo::TXX];
+        mp.zz = w.maps[a][fomo::TZZ];
+        mp.xz = w.maps[a][fomo::TXZ];
+        mp.vx = w.pmaps[a][fomo::VX];
+        mp.vz = w.pmaps[a][fomo::VZ];
+        mp.b0 = m.buoy_maps[0];
+        mp.b1 = m.buoy_maps[1];
+        mp.b2 = m.buoy_maps[2];
+        mp.b3 = m.buoy_maps[3];
+        mp.lam = m.mod_maps[0];
+        mp.mu = m.mod_maps[1];
+        mp.mxz = m.mod_maps[2];
+        if (prof && prof->add(C.stream, 4)) return fail(FOMO_ECUDA, "profiling event failed");
+        CUDA_TRY(fomo::march_launch<M>(A.n_items + (P.rec_k ? rec_blocks : 0), C.stream, P, A, mp));
+        if (prof && prof->end(C.stream)) return fail(FOMO_ECUDA, "profiling event failed");
+        s.launches += 1;
+        w.cur = b;
+        if (k >= 2) s.recorded = k - 1;
+        s.k_done = k;
+    }
+    nvtxRangePop();
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaEventRecord(C.ev1, C.stream));
+    CUDA_TRY(cudaEventSynchronize(C.ev1));
+    float ms = 0;
+    CUDA_TRY(cudaEventElapsedTime(&ms, C.ev0, C.ev1));
+    s.device_ms += ms;
+    return check_status();
+}
+
+// The fused step's plan for a shot, or !ok (split launches): FOMO_STEP_SPLIT,
+// M > 4, or a layout march_plan rejects.
+template <int M>
+MarchPlan shot_march_plan(const Shot& s, const Medium& m) {
+    MarchPlan p;
+    if (g_step_mode.load() == FOMO_STEP_SPLIT) {
+        std::snprintf(p.why, sizeof(p.why), "split launches selected");
+        return p;
+    }
+    if constexpr (M <= 4) {
+        return march_plan<M>(m.nx, m.nz, s.nbc, m.fs != 0, march_slots<M>(), g_march_segs.load());
+    } else {
+        std::snprintf(p.why, sizeof(p.why), "M=%d above the fused step's 4", M);
+        return p;
+    }
+}
+
 template <int M>
 int run_steps_M(Shot& s, Medium& m, Wavefield& w, int n_steps, Profile* prof) {
+    {
+        const MarchPlan plan = shot_march_plan<M>(s, m);
+        if (plan.ok) {
+            if constexpr (M <= 4) return run_steps_march<M>(s, m, w, n_steps, prof, plan);
+        } else if (g_step_mode.load() == FOMO_STEP_FUSED) {
+            return fail(FOMO_EINVAL, "the fused step does not support this shot: %s", plan.why);
+        }
+    }
     auto& C = ctx();
     const bool iso = s.dtx == s.dtz;
     const Launch L = launch_shape<M>(m.nx, m.nz, s.nbc, iso, m.fs != 0);
@@ -993,6 +1184,7 @@ int fomo_b200_shot_profile(uint64_t shot_handle, int32_t n_steps, FomoKernelTime
     if (!s) return fail(FOMO_EINVAL, "unknown shot handle %llu", (unsigned long long)shot_handle);
     if (n_steps < 0 || n_steps > 100000 || !out || !n_kinds || max_kinds < 4)
         return fail(FOMO_EINVAL, "bad profile arguments (max_kinds must be >= 4)");
+    const int nk = max_kinds >= 5 ? 5 : 4;
     Medium* m = get<Medium>(s->medium);
     if (!m) return fail(FOMO_EINVAL, "shot refers to a destroyed medium");
     Profile prof;
@@ -1004,10 +1196,16 @@ int fomo_b200_shot_profile(uint64_t shot_handle, int32_t n_steps, FomoKernelTime
     // and writes txx, tzz, txz (44 B/cell).  Band passes, over the nbc*nx
     // band cells: read the stencil value and the step-start value of each
     // output field and write its final value (24 B/cell velocity, 36 stress).
+    // The fused step reads the five fields, two buoyancy arrays (four when
+    // dx != dz) and lam, mu_txx, mu_txz, and writes the five fields
+    // (60 B/cell, 68 B with four buoyancy arrays).
     const double cells = (double)m->nx * m->nz, band = (double)s->nbc * m->nx;
-    const char* names[4] = {"velocity", "stress", "band_velocity", "band_stress"};
-    const double bytes[4] = {36.0 * cells, 44.0 * cells, 24.0 * band, 36.0 * band};
-    for (int k = 0; k < 4; ++k) {
+    const char* names[5] = {"velocity", "stress", "band_velocity", "band_stress", "step"};
+    const double bytes[5] = {36.0 * cells, 44.0 * cells, 24.0 * band, 36.0 * band,
+                             (s->dtx == s->dtz ? 60.0 : 68.0) * cells};
+    for (size_t i = 0; i < prof.kind.size(); ++i)
+        if (prof.kind[i] >= nk) return fail(FOMO_EINVAL, "the fused step ran: max_kinds must be >= 5");
+    for (int k = 0; k < nk; ++k) {
         std::memset(&out[k], 0, sizeof(FomoKernelTime));
         std::snprintf(out[k].name, sizeof(out[k].name), "%s", names[k]);
         out[k].bytes_per_launch = bytes[k];
@@ -1018,7 +1216,17 @@ int fomo_b200_shot_profile(uint64_t shot_handle, int32_t n_steps, FomoKernelTime
         out[prof.kind[i]].launches += 1;
         out[prof.kind[i]].total_ms += ms;
     }
-    *n_kinds = 4;
+    *n_kinds = nk;
+    return FOMO_OK;
+}
+
+int fomo_b200_set_step_kernel(int32_t mode, int32_t n_segs) {
+    if (mode != FOMO_STEP_AUTO && mode != FOMO_STEP_SPLIT && mode != FOMO_STEP_FUSED)
+        return fail(FOMO_EINVAL, "unknown step kernel mode %d", mode);
+    if (n_segs < 0 || n_segs > fomo::kMMaxSegs)
+        return fail(FOMO_EINVAL, "n_segs=%d out of range 0..%d", n_segs, fomo::kMMaxSegs);
+    g_step_mode.store(mode);
+    g_march_segs.store(n_segs);
     return FOMO_OK;
 }
 

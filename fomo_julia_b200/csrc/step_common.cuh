@@ -72,6 +72,22 @@ __device__ __forceinline__ const float* in_field(const StepParams& P, int q) {
     return p;
 }
 
+// P.out[q] and P.w_tab[t] for indices known only at run time, as selects.
+__device__ __forceinline__ float* out_field(const StepParams& P, int q) {
+    float* p = P.out[0];
+    p = q == 1 ? P.out[1] : p;
+    p = q == 2 ? P.out[2] : p;
+    p = q == 3 ? P.out[3] : p;
+    p = q == 4 ? P.out[4] : p;
+    return p;
+}
+__device__ __forceinline__ const float* w_table(const StepParams& P, int t) {
+    const float* p = P.w_tab[0];
+    p = t == 1 ? P.w_tab[1] : p;
+    p = t == 2 ? P.w_tab[2] : p;
+    return p;
+}
+
 // ---------------------------------------------------------------------------
 // Stencils.  The explosive source (txx, tzz += w at the source cell,
 // source_receiver.jl:26-27) is applied to the values read, never stored, so

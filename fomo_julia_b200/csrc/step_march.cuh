@@ -7,14 +7,14 @@
 // for M <= 4) and each strip into row segments; one block owns one
 // (strip, segment) and marches down it in blocks of kMR = 16 rows.  At
 // iteration t it computes
-//   velocity block t   rows za - M + 16t .. +16, over the strip plus an HV-column
-//                      halo on each side (64 columns: the stress of the
-//                      strip's edge columns reads them), and
+//   velocity block t   rows za - M + 16t .. +16, over the strip plus an
+//                      HV-column halo on each side (64 columns: the stress
+//                      of the strip's edge columns reads them), and
 //   stress block t-1   rows za + 16(t-1) .. +16, over the strip's own columns,
 // from velocity blocks t-1 and t, which stay in a shared-memory ring of three
-// blocks.  New velocities never go back to HBM before the stress reads them,
-// and neither the velocity halo nor the rows above a segment cost DRAM reads
-// beyond the tau boxes' overlap (served by L2).
+// blocks.  New velocities never go back to HBM before the stress reads them;
+// the velocity halo and the rows above a segment are recomputed, and the tau
+// boxes' overlap is served by L2.
 //
 // Data movement.  Thread 0 loads each iteration's tau box (txx, tzz, txz over
 // 72 x (16 + 2M) cells: the velocity stencil's inputs and the stress's
@@ -27,18 +27,16 @@
 // Boundary rules, all inside the march:
 //   left/right HABC (boundary.jl:76-85): strips whose columns reach a band
 //     exchange their pre-HABC values through shared memory and apply the
-//     rules of step_common.cuh; the first strip holds the whole left band and
-//     the column its rule reads, the last (right-aligned) strip the whole
-//     right band and the two columns its rules read;
+//     rules of step_common.cuh; the host's plan (march_plan) admits a layout
+//     only if every rule a strip needs reads columns the strip computes;
 //   bottom band and corners (boundary.jl:88-132): a recurrence along j; the
 //     blocks that hold band rows march them in order, one warp per 28-column
-//     strip and field, exactly as band_march does (lane rules, shuffles);
+//     strip and field, with band_march's lane rules and shuffles;
 //   free surface (boundary.jl:168-181): tzz = txz = 0 in rows pad-5..pad;
 //   source (source_receiver.jl:18-30): added to the smem copy of a tau box;
 //   receivers (source_receiver.jl:65-77): record blocks appended to the grid
 //     read the step-start copy, as in the split launches.
-// The fused step needs a free surface (no top HABC band), M <= 4 and bands
-// narrow enough for the first and last strips (march_supported); other
+// The fused step needs a free surface (no top HABC band) and M <= 4; other
 // configurations run the split launches.
 #pragma once
 
@@ -60,11 +58,10 @@ struct MGeo {
     static constexpr int W = kMVW - 2 * HV;         // output columns of a strip
     static constexpr int TW = kMVW + 2 * HV;        // tau box width
     static constexpr int TH = kMR + 2 * M;          // tau box rows
-    static constexpr int TAU = TW * TH;             // floats of one field's box
+    static constexpr int TAU = (TW * TH + 31) / 32 * 32;  // floats of one field's box (128-byte multiple)
     static constexpr int STAGE = 3 * TAU;
     static constexpr int RING_ROWS = kMRing * kMR;  // 48
     static constexpr int RING = RING_ROWS * kMVW;   // floats of one field's ring
-    static constexpr int NQ = 3;                    // float4s of an x window (HV = 4)
 };
 
 // Launch-wide parameters of the fused step (besides StepParams).
@@ -92,7 +89,7 @@ __host__ __device__ constexpr size_t march_smem_floats() {
     return (size_t)kMStages * G::STAGE + 2 * (size_t)G::RING + 3 * kMVW;
 }
 template <int M>
-__host__ constexpr size_t march_smem_bytes() {
+__host__ __device__ constexpr size_t march_smem_bytes() {
     return march_smem_floats<M>() * 4 + kMStages * 8 + 16;
 }
 
@@ -158,7 +155,8 @@ __device__ __forceinline__ float4 mul4s(float4 a, float s) {
 }
 
 // Values of one field over a shared-memory row-major region whose row r0
-// holds grid row z0 and column 0 grid column xs (rows wrap after `rows`).
+// holds grid row z0 and whose column 0 is grid column xs (rows wrap after
+// `rows`).
 struct SmemRows {
     const float* base;
     int xs, z0, r0, rows, pitch;
@@ -173,10 +171,10 @@ struct SmemRows {
 // band rows [ja, jb) of one block: `pre` holds the block's values after the
 // stencil update (band rows) and final values (rows above), and receives the
 // finals in place.  One warp per 28-column strip: lane l holds column
-// xs - 2 + l; lanes 2..29 write back and store (own columns only).  The lane
-// rules are band_march's.
-// `prev` (column 0 = pre_xs), when given, holds the finals of row ja - 1;
-// otherwise that row is read from `pre`.
+// xs - 2 + l; lanes 2..29 write back, and store their own columns
+// [own_lo, own_hi).  Columns [c_lo, c_hi) hold values.  `prev` (column 0 =
+// pre_xs), when given, holds the finals of row ja - 1; otherwise that row is
+// read from `pre`.  The lane rules are band_march's.
 __device__ __forceinline__ void march_band_rows(const StepParams& P, const float* tab, const float* oin, float* oout,
                                                 float* pre, int pre_pitch, int pre_xs, int pre_z0, int pre_r0,
                                                 int pre_rows, int c_lo, int c_hi, int own_lo, int own_hi, int xs,
@@ -250,14 +248,14 @@ __global__ void __launch_bounds__(kMThreads, 2)
 
     float* stage = smem;
     float* ring = smem + kMStages * G::STAGE;          // [2 fields][48 rows][64]
-    float* s_last = ring + 2 * G::RING;                // [3][64] stress finals of the last row of a block
+    float* s_last = ring + 2 * G::RING;                // [3][64] stress finals of a block's last row
     uint64_t* full = reinterpret_cast<uint64_t*>(s_last + 3 * kMVW);
 
     auto issue = [&](int t) {
         const int s = t % kMStages;
         float* dst = stage + s * G::STAGE;
         const int vr0 = za - M + t * kMR;
-        mbar_expect_tx(full + s, 3 * G::TAU * 4);
+        mbar_expect_tx(full + s, 3 * G::TW * G::TH * 4);  // the bytes of the three boxes
         tma_load_2d(dst, &mp.xx, x0 - 2 * G::HV, vr0 - M, full + s);
         tma_load_2d(dst + G::TAU, &mp.zz, x0 - 2 * G::HV, vr0 - M, full + s);
         tma_load_2d(dst + 2 * G::TAU, &mp.xz, x0 - 2 * G::HV, vr0 - M, full + s);
@@ -294,8 +292,8 @@ __global__ void __launch_bounds__(kMThreads, 2)
         const int s = t % kMStages;
         float* tau = stage + s * G::STAGE;
         if (!mbar_wait_parity(full + s, (t / kMStages) & 1, A.status)) return;
-        // ------------------------------------------------ the source, into this stage's copy
         const int vr0 = za - M + t * kMR;
+        // ------------------------------------------------ the source, into this stage's copy
         {
             const int si = P.src_i - (x0 - 2 * G::HV), sj = P.src_j - (vr0 - M);
             if (si >= 0 && si < G::TW && sj >= 0 && sj < G::TH) {  // block-uniform
@@ -309,7 +307,7 @@ __global__ void __launch_bounds__(kMThreads, 2)
         // ------------------------------------------------ velocity block t
         {
             const int j = vr0 + ty;
-            // rows the stress of this segment reads: the last block feeds 2M stress rows
+            // rows the stress of this segment reads (the last block feeds 2M stress rows)
             const int v_hi = min(vr0 + (t < n_it - 1 ? kMR : 2 * M), zb + M);
             float4 ox = make_float4(0.f, 0.f, 0.f, 0.f), oz = ox;
             const bool row_ok = j < v_hi && j >= 0 && j < nz;
@@ -318,7 +316,7 @@ __global__ void __launch_bounds__(kMThreads, 2)
                 const float4 vx = ldg4(P.in[VX] + c), vz = ldg4(P.in[VZ] + c);
                 const float4 b0 = ldg4(A.b[0] + c), b2 = ldg4(A.b[2] + c);
                 const float4 b1 = A.iso ? b0 : ldg4(A.b[1] + c), b3 = A.iso ? b2 : ldg4(A.b[3] + c);
-                const float* rxx = tau + (ty + M) * G::TW + 4 * tx;             // window from column xv - 4
+                const float* rxx = tau + (ty + M) * G::TW + 4 * tx;  // windows from column xv - 4
                 const float* rxz = tau + 2 * G::TAU + (ty + M) * G::TW + 4 * tx;
                 const float4 d1 = xderiv1<M, 0>(P, rxx);   // dtxx/dx: txx[i+l-1] - txx[i-l]
                 const float4 d3 = xderiv1<M, 1>(P, rxz);   // dtxz/dx: txz[i+l] - txz[i-l+1]
@@ -356,9 +354,9 @@ __global__ void __launch_bounds__(kMThreads, 2)
 #pragma unroll
                     for (int c4 = 0; c4 < 4; ++c4) {
                         const int i = xv + c4;
-                        // the rule's neighbours must lie in the strip's columns
-                        if (i > xa && i < xa + kMVW - 1 && lr_band_cell(P, i, j) &&
-                            (i <= b || i - 2 >= xa)) {
+                        // the rule's neighbours (left: i+1; right: i-1, i-2) lie in the strip's
+                        // columns for every cell the stress reads (march_plan checks it)
+                        if (lr_band_cell(P, i, j) && (i <= b ? i + 1 < xa + kMVW : i - 2 >= xa)) {
                             set_comp(ox, c4, hx.final_value(i, j));
                             set_comp(oz, c4, hz.final_value(i, j));
                         }
@@ -371,16 +369,19 @@ __global__ void __launch_bounds__(kMThreads, 2)
                     __syncthreads();
                     if (warp < 6) {
                         const int f = warp / 3, ws = warp % 3;
-                        march_band_rows(P, P.w_tab[f], P.in[VX + f], P.out[VX + f], ring + f * G::RING, kMVW, xa,
-                                        vr0, (t % kMRing) * kMR, G::RING_ROWS, xa, xa + kMVW, x0, x_end,
-                                        xa + 28 * ws, max(vr0, j0), min(v_hi, nz - 1), nullptr);
+                        march_band_rows(P, w_table(P, f), in_field(P, VX + f), out_field(P, VX + f),
+                                        ring + f * G::RING, kMVW, xa, vr0, (t % kMRing) * kMR, G::RING_ROWS, xa,
+                                        xa + kMVW, x0, x_end, xa + 28 * ws, max(vr0, j0), min(v_hi, nz - 1),
+                                        nullptr);
                     }
                     __syncthreads();
                     ox = *reinterpret_cast<const float4*>(rvx);
                     oz = *reinterpret_cast<const float4*>(rvz);
                 }
             }
-            if (row_ok && v_own && !(j >= j0 && j <= nz - 2)) {  // band rows were stored by the march
+            // the segment's own rows (the rows above are the previous segment's); band rows were
+            // stored by the march
+            if (row_ok && v_own && j >= za && j < zb && !(j >= j0 && j <= nz - 2)) {
                 stg4(P.out[VX] + cell(P, xv, j), ox);
                 stg4(P.out[VZ] + cell(P, xv, j), oz);
             }
@@ -401,9 +402,10 @@ __global__ void __launch_bounds__(kMThreads, 2)
                 const size_t c = cell(P, xs, j);
                 const float4 lam = ldg4(P.lam + c), mu = ldg4(P.mu_txx + c), mxz = ldg4(P.mu_txz + c);
                 const int bo = (ty + 2 * M) * G::TW + 2 * G::HV + 4 * tx;
-                const float4 txx = lds4(told + bo), tzz = lds4(told + G::TAU + bo), txz = lds4(told + 2 * G::TAU + bo);
-                // ring row of grid row j - M (relative row (t-1)*16 + ty)
-                int r = (((t - 1) % kMRing) * kMR + ty);
+                const float4 txx = lds4(told + bo), tzz = lds4(told + G::TAU + bo);
+                const float4 txz = lds4(told + 2 * G::TAU + bo);
+                // ring row of grid row j - M is r (relative row (t-1)*16 + ty, modulo the ring)
+                const int r = ((t - 1) % kMRing) * kMR + ty;
                 const float* rvx = ring + 4 * tx;
                 const float* rvz = ring + G::RING + 4 * tx;
                 const float4 dxx = xderiv1<M, 1>(P, rvx + (r + M) % G::RING_ROWS * kMVW);  // vx[i+l] - vx[i-l+1]
@@ -451,7 +453,7 @@ __global__ void __launch_bounds__(kMThreads, 2)
 #pragma unroll
                     for (int c4 = 0; c4 < 4; ++c4) {
                         const int i = xs + c4;
-                        if (i >= x0 && i < x0 + G::W - 1 && lr_band_cell(P, i, j) && (i <= b || i - 2 >= x0)) {
+                        if (lr_band_cell(P, i, j) && (i <= b ? i + 1 < x0 + G::W : i - 2 >= x0)) {
                             set_comp(oxx, c4, h0.final_value(i, j));
                             set_comp(ozz, c4, h1.final_value(i, j));
                             set_comp(oxz, c4, h2.final_value(i, j));
@@ -470,9 +472,9 @@ __global__ void __launch_bounds__(kMThreads, 2)
                     if (warp < 6) {
                         const int f = warp / 2, ws = warp % 2;
                         // the row above the first band row: in this block, or the previous block's last row
-                        march_band_rows(P, P.w_tab[2], P.in[TXX + f], P.out[TXX + f], sp + f * kMR * kMVW, kMVW, x0,
-                                        sr0, 0, kMR, x0, x0 + G::W, x0, x_end, x0 + 28 * ws, ja, jb,
-                                        ja == sr0 ? s_last + f * kMVW : nullptr);
+                        march_band_rows(P, P.w_tab[2], in_field(P, TXX + f), out_field(P, TXX + f),
+                                        sp + f * kMR * kMVW, kMVW, x0, sr0, 0, kMR, x0, x0 + G::W, x0, x_end,
+                                        x0 + 28 * ws, ja, jb, ja == sr0 ? s_last + f * kMVW : nullptr);
                     }
                     __syncthreads();
                     if (s_col) {
@@ -482,21 +484,19 @@ __global__ void __launch_bounds__(kMThreads, 2)
                     }
                 }
             }
-            if (row_ok && s_own) {
-                if (in_free_surface_rows(P, j)) {
-                    ozz = make_float4(0.f, 0.f, 0.f, 0.f);
-                    oxz = ozz;
-                }
-                if (!(j >= j0 && j <= nz - 2)) {
-                    stg4(P.out[TXX] + cell(P, xs, j), oxx);
-                    stg4(P.out[TZZ] + cell(P, xs, j), ozz);
-                    stg4(P.out[TXZ] + cell(P, xs, j), oxz);
-                }
-            }
             if (ty == kMR - 1 && s_col) {  // the block's last row, read by the next block's band march
                 *reinterpret_cast<float4*>(s_last + 4 * tx) = oxx;
                 *reinterpret_cast<float4*>(s_last + kMVW + 4 * tx) = ozz;
                 *reinterpret_cast<float4*>(s_last + 2 * kMVW + 4 * tx) = oxz;
+            }
+            if (row_ok && s_own && !(j >= j0 && j <= nz - 2)) {  // band rows were stored by the march
+                if (in_free_surface_rows(P, j)) {
+                    ozz = make_float4(0.f, 0.f, 0.f, 0.f);
+                    oxz = ozz;
+                }
+                stg4(P.out[TXX] + cell(P, xs, j), oxx);
+                stg4(P.out[TZZ] + cell(P, xs, j), ozz);
+                stg4(P.out[TXZ] + cell(P, xs, j), oxz);
             }
         }
     }

@@ -207,7 +207,7 @@ __device__ __forceinline__ bool wait_tma(uint64_t* bar, const TiledArgs& T) {
 // Self-test of the bounded wait: thread 0 arms an mbarrier for a byte count
 // that no copy delivers and waits `limit` polls on it, exactly as a tile
 // waits for its TMA boxes; no memory operation is outstanding.
-__global__ void wait_selftest_kernel(int* status, int limit) {
+static __global__ void wait_selftest_kernel(int* status, int limit) {
     __shared__ __align__(8) uint64_t bar;
     if (threadIdx.x != 0) return;
     mbar_init(&bar, 1);
@@ -833,7 +833,7 @@ __global__ void __launch_bounds__(kThreads, kTileBlocks<M>) stress_kernel(const 
 }
 
 // Receivers of the last step (the velocity launch of step k records k-1).
-__global__ void record_kernel(const StepParams P) { record_block(P, blockIdx.x, P.rec_k); }
+static __global__ void record_kernel(const StepParams P) { record_block(P, blockIdx.x, P.rec_k); }
 
 // ---------------------------------------------------------------- bottom band
 // Rows nz-nbc-1 .. nz-2: the bottom edge and the two bottom corners, whose
@@ -957,7 +957,7 @@ __global__ void __launch_bounds__(32) band_kernel(const __grid_constant__ StepPa
 //   kind 0  p   = (txx + tzz) * 0.5
 //   kind 1  vel = sqrt(vx^2 + vz^2)
 //   kind 2  vx,   kind 3  vz.
-__global__ void snapshot_kernel(const float* f0, const float* f1, int kind, int nx, int nz, int pitch, int ds,
+static __global__ void snapshot_kernel(const float* f0, const float* f1, int kind, int nx, int nz, int pitch, int ds,
                                 int nx_d, int nz_d, float* out) {
     const size_t n = (size_t)nx_d * nz_d;
     for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
@@ -996,7 +996,7 @@ struct ModelView {
     }
 };
 
-__global__ void medium_init_kernel(const ModelView V, int nx, int nz, int pitch, float* rho_vx, float* rho_vz,
+static __global__ void medium_init_kernel(const ModelView V, int nx, int nz, int pitch, float* rho_vx, float* rho_vz,
                                    float* lam, float* mu_txx, float* mu_txz) {
     const size_t n = (size_t)nx * nz;
     for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
@@ -1017,7 +1017,7 @@ __global__ void medium_init_kernel(const ModelView V, int nx, int nz, int pitch,
 
 // Buoyancy dtx/rho_vx, dtz/rho_vx, dtx/rho_vz, dtz/rho_vz: the divisions of
 // update_velocity! (velocity.jl:41-42), IEEE-rounded, once per medium and dt.
-__global__ void buoyancy_kernel(const float* rho_vx, const float* rho_vz, float dtx, float dtz, size_t n,
+static __global__ void buoyancy_kernel(const float* rho_vx, const float* rho_vz, float dtx, float dtz, size_t n,
                                 float* b0, float* b1, float* b2, float* b3) {
     for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
         const float rx = rho_vx[k], rz = rho_vz[k];

@@ -91,6 +91,19 @@ def synchronize(b: B200Backend = B200_BACKEND) -> None:
     call("fomo_b200_synchronize")
 
 
+STEP_KERNELS = {"auto": 0, "split": 1, "fused": 2}
+
+
+def set_step_kernel(mode: str = "auto", n_segs: int = 0) -> None:
+    """Time-step kernels of single shots (no reference counterpart): "auto"
+    runs the fused step (one launch per step) wherever it supports the shot
+    and the split launches elsewhere; "split" always runs the split launches;
+    "fused" makes a shot the fused step cannot run fail.  n_segs > 0 fixes
+    the fused step's row segments per column strip.  Results are the same bit
+    for bit."""
+    call("fomo_b200_set_step_kernel", STEP_KERNELS[mode], int(n_segs))
+
+
 # ---------------------------------------------------------------------------
 # Initialisation  (src/utils/init.jl)
 # ---------------------------------------------------------------------------

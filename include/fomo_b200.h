@@ -221,7 +221,8 @@ int fomo_b200_shot_finish(uint64_t shot_handle, float* gather_out, FomoRunStats*
 /* Per-kernel timing of a shot's loop (no reference counterpart; used by
  * bench.py for the roofline).  Runs up to n_steps more steps of the shot
  * with CUDA events around every launch and reports, per kernel kind
- * (velocity, stress, band_velocity, band_stress: max_kinds >= 4), the
+ * (velocity, stress, band_velocity, band_stress: max_kinds >= 4; and step,
+ * the fused step, when max_kinds >= 5), the
  * launches, their summed device time and the algorithmic DRAM bytes of one
  * launch (the bytes a launch must move at minimum: each array it reads
  * once and each array it writes once, over the cells it updates). */
@@ -234,6 +235,23 @@ typedef struct {
 
 int fomo_b200_shot_profile(uint64_t shot_handle, int32_t n_steps, FomoKernelTime* out,
                            int32_t max_kinds, int32_t* n_kinds);
+
+/* Time-step kernel selection (no reference counterpart; a tuning control).
+ * FOMO_STEP_AUTO runs the fused step -- one launch per time step that
+ * computes velocity and stress together, so every field and medium array
+ * crosses HBM once -- wherever it supports the shot (free surface, M <= 4,
+ * HABC bands that fit its first and last column strips) and the split
+ * launches (velocity, band pass, stress, band pass) elsewhere;
+ * FOMO_STEP_SPLIT always runs the split launches; FOMO_STEP_FUSED fails a
+ * single shot that the fused step does not support with FOMO_EINVAL.
+ * n_segs > 0 fixes the fused step's row segments per column strip (1..64;
+ * 0 = chosen from the grid and the SM count).  Process-wide; results are
+ * bit-identical either way.  The batched and served paths and
+ * fomo_b200_run_shot_noalloc use the split launches. */
+#define FOMO_STEP_AUTO 0
+#define FOMO_STEP_SPLIT 1
+#define FOMO_STEP_FUSED 2
+int fomo_b200_set_step_kernel(int32_t mode, int32_t n_segs);
 
 /* Self-test of the kernels' bounded device waits (no reference
  * counterpart).  Every wait of a time-step kernel on its TMA loads polls at

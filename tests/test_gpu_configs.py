@@ -74,11 +74,20 @@ def test_small_homogeneous_full_shot(rec_type, b200, oracle_lib):
     _assert_bit_exact(r.gather, g_orc, f_gpu, f_orc)
 
 
-def test_large_layered_first_steps(b200, oracle_lib):
+@pytest.fixture(params=["auto", "split"])
+def step_mode(request):
+    """The fused step ("auto" picks it on these workloads) and the split launches."""
+    F.set_step_kernel(request.param)
+    yield request.param
+    F.set_step_kernel("auto")
+
+
+def test_large_layered_first_steps(b200, oracle_lib, step_mode):
     n = 60
     w = synthetic.large_layered()
     c = case_from_workload(w)
     r, f_gpu = _gpu(c, b200, n_steps=n)
+    assert (r.stats["kernel_launches"] <= n + 1) == (step_mode == "auto")
     assert r.stats["steps"] == n
     g_orc, f_orc = _oracle(c, oracle_lib, n_steps=n)
     assert (r.gather.shape, f_gpu["vx"].shape) == ((11520, 1000), (4552, 3927))
@@ -87,7 +96,7 @@ def test_large_layered_first_steps(b200, oracle_lib):
 
 
 @pytest.mark.parametrize("shot", [0, 33])
-def test_batched_medium_single_shots(shot, b200, oracle_lib):
+def test_batched_medium_single_shots(shot, b200, oracle_lib, step_mode):
     n = 300
     w = synthetic.batched_layered()
     c = case_from_workload(w, shot=shot, nt=n)

@@ -106,12 +106,69 @@ CASES = [
 ]
 
 
+def fused_supported(c: Case) -> bool:
+    """Shots the fused step (one launch per step) runs: free surface, order
+    <= 8, and HABC bands that fit its first and last column strips."""
+    return c.free_surface and c.fd_order <= 8 and c.nbc <= 50
+
+
+@pytest.fixture
+def step_kernel():
+    """Selects the time-step kernels for one test and restores "auto"."""
+    yield F.set_step_kernel
+    F.set_step_kernel("auto")
+
+
 @pytest.mark.parametrize("c", CASES, ids=lambda c: c.name)
 def test_shot_matches_oracle(c, b200, oracle_lib):
+    # "auto": the fused step where it applies, the split launches elsewhere
     r, f_gpu = gpu_run(c, b200)
     g_orc, f_orc = oracle_run(c, oracle_lib)
     assert_same(r.gather, g_orc, f_gpu, f_orc)
     assert r.stats["steps"] == c.nt
+    launches_per_step = r.stats["kernel_launches"] / c.nt
+    assert (launches_per_step < 1.5) == fused_supported(c), launches_per_step
+
+
+@pytest.mark.parametrize("c", [c for c in CASES if fused_supported(c)], ids=lambda c: c.name)
+def test_split_launches_match_oracle(c, b200, oracle_lib, step_kernel):
+    # the same shots through the split launches (velocity, band pass, stress, band pass)
+    step_kernel("split")
+    r, f_gpu = gpu_run(c, b200)
+    g_orc, f_orc = oracle_run(c, oracle_lib)
+    assert_same(r.gather, g_orc, f_gpu, f_orc)
+    assert r.stats["kernel_launches"] >= 4 * c.nt
+
+
+SEGMENT_CASES = [
+    (layered(231, 190, seed=61, nbc=10, fd_order=8, nt=120, n_rec=41), 2),
+    (layered(231, 190, seed=61, nbc=10, fd_order=8, nt=120, n_rec=41), 5),
+    (layered(150, 260, seed=62, nbc=12, fd_order=4, nt=110, rec_type="p", water_rows=5), 7),
+    (layered(190, 240, seed=63, nbc=20, fd_order=6, nt=100, rec_type="vx"), 3),
+    (layered(170, 220, seed=64, nbc=7, fd_order=2, nt=100), 4),
+    (layered(120, 300, seed=65, nbc=50, fd_order=8, nt=100, n_rec=9), 6),
+]
+
+
+@pytest.mark.parametrize("c,n_segs", SEGMENT_CASES,
+                         ids=[f"{c.name}-segs{n}" for c, n in SEGMENT_CASES])
+def test_fused_step_row_segments(c, n_segs, b200, oracle_lib, step_kernel):
+    # row segments of the fused step recompute the velocity rows above them
+    step_kernel("fused", n_segs)
+    r, f_gpu = gpu_run(c, b200)
+    g_orc, f_orc = oracle_run(c, oracle_lib)
+    assert_same(r.gather, g_orc, f_gpu, f_orc)
+    assert r.stats["kernel_launches"] <= c.nt + 1
+
+
+def test_fused_step_refuses_what_it_cannot_run(b200, step_kernel):
+    step_kernel("fused")
+    no_fs = layered(36, 31, seed=4, nbc=6, fd_order=8, free_surface=False, nt=5)
+    with pytest.raises(F._lib.FomoError, match="FOMO_EINVAL.*fused step"):
+        gpu_run(no_fs, b200)
+    order12 = layered(41, 27, seed=3, nbc=7, fd_order=12, nt=5)
+    with pytest.raises(F._lib.FomoError, match="FOMO_EINVAL.*fused step"):
+        gpu_run(order12, b200)
 
 
 def test_shot_1_golden(b200, oracle_lib):

@@ -11,6 +11,7 @@ namespace fomo {
 struct StepParams;
 struct MarchArgs;
 struct MarchMaps;
+struct BatchMarchLaunch;
 
 // Launches march_kernel<M> with `blocks` blocks on `st`.
 template <int M>
@@ -20,11 +21,21 @@ cudaError_t march_launch(int blocks, cudaStream_t st, const StepParams& P, const
 template <int M>
 const void* march_kernel_fn();
 
+// Launches batch_march_kernel<M> (many shots per launch) with `blocks` blocks.
+template <int M>
+cudaError_t batch_march_launch(int blocks, cudaStream_t st, const BatchMarchLaunch& L);
+template <int M>
+const void* batch_march_kernel_fn();
+
 #define FOMO_MARCH_DECLARE(M)                                                                              \
     template <>                                                                                            \
     cudaError_t march_launch<M>(int, cudaStream_t, const StepParams&, const MarchArgs&, const MarchMaps&); \
     template <>                                                                                            \
-    const void* march_kernel_fn<M>();
+    const void* march_kernel_fn<M>();                                                                      \
+    template <>                                                                                            \
+    cudaError_t batch_march_launch<M>(int, cudaStream_t, const BatchMarchLaunch&);                         \
+    template <>                                                                                            \
+    const void* batch_march_kernel_fn<M>();
 FOMO_MARCH_DECLARE(1)
 FOMO_MARCH_DECLARE(2)
 FOMO_MARCH_DECLARE(3)

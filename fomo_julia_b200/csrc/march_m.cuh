@@ -19,4 +19,15 @@ const void* march_kernel_fn<FOMO_MARCH_M>() {
     return reinterpret_cast<const void*>(&march_kernel<FOMO_MARCH_M>);
 }
 
+template <>
+cudaError_t batch_march_launch<FOMO_MARCH_M>(int blocks, cudaStream_t st, const BatchMarchLaunch& L) {
+    batch_march_kernel<FOMO_MARCH_M><<<blocks, kMThreads, march_smem_bytes<FOMO_MARCH_M>(), st>>>(L);
+    return cudaGetLastError();
+}
+
+template <>
+const void* batch_march_kernel_fn<FOMO_MARCH_M>() {
+    return reinterpret_cast<const void*>(&batch_march_kernel<FOMO_MARCH_M>);
+}
+
 }  // namespace fomo

@@ -110,6 +110,8 @@ struct Request {
     int start = 0;           // batch step of the shot's step 1
     size_t band_off = 0, tabs_off = 0, cells_off = 0, wav_off = 0, gather_off = 0;
     fomo::BatchShot vel, str;  // the shot's launch-parameter images (velocity, stress)
+    fomo::MarchShot march;     // and of the fused step (all five fields of copy c to copy 1-c)
+    bool fused = false;        // runs in a fused-step launch set
     CUtensorMap halo[2][5];  // halo boxes (Geo<M>) of every field of both copies
     CUtensorMap tile[2][5];  // tile boxes of every field of both copies
     void* staging = nullptr; // pinned: gather + status word
@@ -212,6 +214,84 @@ struct LaunchSet {
     int grid_v = 0, grid_s = 0, grid_b = 0;    // velocity tiles + receivers, stress tiles, band passes
     size_t smem_v = 0, smem_s = 0;
 };
+
+// Shots of one FD order in flight that run the fused step: one launch per
+// batch step.
+struct MarchSet {
+    int M = 0;
+    std::shared_ptr<fomo::BatchMarchLaunch> L;
+    int grid = 0;
+};
+
+template <int M>
+int march_plan_for(int nx, int nz, int nbc, bool fs, int slots, MarchPlan* out) {
+    if constexpr (M <= 4) {
+        *out = march_plan<M>(nx, nz, nbc, fs, slots, g_march_segs.load());
+        return FOMO_OK;
+    } else {
+        return FOMO_EINVAL;
+    }
+}
+
+// The fused-step plan of a request's grid with `slots` blocks to fill.
+MarchPlan request_march_plan(const Medium& m, int nbc, int M, int slots) {
+    MarchPlan p;
+    switch (M) {
+        case 1: march_plan_for<1>(m.nx, m.nz, nbc, m.fs != 0, slots, &p); break;
+        case 2: march_plan_for<2>(m.nx, m.nz, nbc, m.fs != 0, slots, &p); break;
+        case 3: march_plan_for<3>(m.nx, m.nz, nbc, m.fs != 0, slots, &p); break;
+        case 4: march_plan_for<4>(m.nx, m.nz, nbc, m.fs != 0, slots, &p); break;
+    }
+    return p;
+}
+
+int march_slots_of(int M) {
+    switch (M) {
+        case 1: return march_slots<1>();
+        case 2: return march_slots<2>();
+        case 3: return march_slots<3>();
+        case 4: return march_slots<4>();
+    }
+    return 2 * sm_count();
+}
+
+size_t march_smem_bytes_any(int M) {
+    switch (M) {
+        case 1: return fomo::march_smem_bytes<1>();
+        case 2: return fomo::march_smem_bytes<2>();
+        case 3: return fomo::march_smem_bytes<3>();
+        case 4: return fomo::march_smem_bytes<4>();
+    }
+    return 0;
+}
+
+cudaError_t batch_march_launch_any(int M, int blocks, cudaStream_t st, const fomo::BatchMarchLaunch& L) {
+    switch (M) {
+        case 1: return fomo::batch_march_launch<1>(blocks, st, L);
+        case 2: return fomo::batch_march_launch<2>(blocks, st, L);
+        case 3: return fomo::batch_march_launch<3>(blocks, st, L);
+        case 4: return fomo::batch_march_launch<4>(blocks, st, L);
+    }
+    return cudaErrorInvalidValue;
+}
+
+const void* batch_march_kernel_any(int M) {
+    switch (M) {
+        case 1: return fomo::batch_march_kernel_fn<1>();
+        case 2: return fomo::batch_march_kernel_fn<2>();
+        case 3: return fomo::batch_march_kernel_fn<3>();
+        case 4: return fomo::batch_march_kernel_fn<4>();
+    }
+    return nullptr;
+}
+
+// A request runs the fused step unless the split launches are selected or
+// the fused step does not support its grid (M > 4, no free surface, HABC
+// bands beyond its edge strips).
+bool march_ok(const Request& r) {
+    if (g_step_mode.load() == FOMO_STEP_SPLIT || r.M > 4) return false;
+    return request_march_plan(*r.med, r.nbc, r.M, march_slots_of(r.M)).ok;
+}
 
 // A set's tile launch of one half step (after_band: a dependent launch
 // beside the band pass just before it, see launch_tiles).
@@ -419,6 +499,8 @@ class Server {
     int64_t k_host_ = 0;          // batch steps enqueued
     bool dirty_ = true;           // membership changed since the tables were built
     std::vector<LaunchSet> sets_;
+    std::vector<MarchSet> msets_;  // fused-step sets (their counters follow the split sets')
+    cudaError_t enqueue_err_ = cudaSuccess;
     std::map<int, cudaGraphExec_t> graphs_;  // K -> graph of the current tables
     std::deque<cudaEvent_t> inflight_;
     std::vector<Deferred> deferred_;
@@ -655,6 +737,20 @@ class Server {
             S->start = r.start;
             S->nt = r.nt;
         }
+        std::memset((void*)&r.march, 0, sizeof(r.march));
+        r.march.wavelet = reinterpret_cast<const float*>(base + r.wav_off);
+        r.march.n_wavelet = (int)r.wavelet.size();
+        r.march.start = r.start;
+        r.march.nt = r.nt;
+        for (int c = 0; c < 2; ++c) {
+            fomo::StepParams& F = r.march.P[c];
+            F = P;
+            for (int q = 0; q < 5; ++q) {
+                F.in[q] = field[c][q];
+                F.out[q] = field[1 - c][q];
+            }
+        }
+        r.fused = march_ok(r);
         for (int c = 0; c < 2; ++c) {  // the step reads copy c, writes copy 1-c
             const int o = 1 - c;
             fomo::StepParams& V = r.vel.P[c];
@@ -675,8 +771,8 @@ class Server {
     // ------------------------------------------------------------ tables
     int build_tables() {
         // Order: by M, then by medium (groups), then admission.
-        std::vector<Request*> order;
-        for (auto& r : active_) order.push_back(r.get());
+        std::vector<Request*> order, fused;
+        for (auto& r : active_) (r->fused ? fused : order).push_back(r.get());
         std::stable_sort(order.begin(), order.end(), [](const Request* x, const Request* y) {
             if (x->M != y->M) return x->M < y->M;
             return x->med < y->med;
@@ -756,7 +852,77 @@ class Server {
             fomo::batch_counters_kernel<<<(n + 255) / 256, 256, 0, st_>>>(d_counters_, n, (int)(k_host_ + 1));
             CUDA_TRY(cudaGetLastError());
         }
+        if (int rc = build_march_sets(fused)) return rc;
         dirty_ = false;
+        return FOMO_OK;
+    }
+
+    // Fused-step sets: by M, then medium and HABC width (one layout per
+    // group), at most kMarchShots shots and kMarchGroups groups per set.
+    int build_march_sets(std::vector<Request*>& order) {
+        std::stable_sort(order.begin(), order.end(), [](const Request* x, const Request* y) {
+            if (x->M != y->M) return x->M < y->M;
+            if (x->med != y->med) return x->med < y->med;
+            return x->nbc < y->nbc;
+        });
+        msets_.clear();
+        for (size_t i = 0; i < order.size();) {
+            MarchSet S;
+            S.M = order[i]->M;
+            S.L = std::make_shared<fomo::BatchMarchLaunch>();
+            fomo::BatchMarchLaunch& L = *S.L;
+            std::memset((void*)&L, 0, sizeof(L));
+            int items = 0, n_groups = 0;
+            size_t j = i;
+            while (j < order.size() && order[j]->M == S.M && n_groups < fomo::kMarchGroups &&
+                   j - i < (size_t)fomo::kMarchShots) {
+                size_t h = j;
+                while (h < order.size() && order[h]->M == S.M && order[h]->med == order[j]->med &&
+                       order[h]->nbc == order[j]->nbc && h - i < (size_t)fomo::kMarchShots)
+                    ++h;
+                const int n = (int)(h - j);
+                const MarchPlan plan =
+                    request_march_plan(*order[j]->med, order[j]->nbc, S.M, std::max(1, march_slots_of(S.M) / n));
+                if (!plan.ok) return fail(FOMO_ECUDA, "fused-step plan lost for a running shot: %s", plan.why);
+                fomo::MarchGroup& G = L.groups[n_groups++];
+                G.A = plan.A;
+                for (int q = 0; q < 4; ++q) G.A.b[q] = order[j]->res->b[q];
+                G.A.iso = order[j]->res->iso;
+                G.A.status = d_status_;
+                G.first = (int)(j - i);
+                G.n = n;
+                G.item_off = items;
+                items += n * plan.A.n_items;
+                j = h;
+            }
+            int rec = 0;
+            L.rec_off[0] = 0;
+            for (size_t k = i; k < j; ++k) {
+                const Request& r = *order[k];
+                const size_t t = k - i;
+                rec += (r.n_rec + fomo::kMThreads - 1) / fomo::kMThreads;
+                L.rec_off[t + 1] = rec;
+                L.shot[t] = r.march;
+                for (int c = 0; c < 2; ++c)
+                    for (int f = 0; f < 3; ++f) L.tau[t][c][f] = r.halo[c][fomo::TXX + f];
+            }
+            int* cnt = d_counters_ + 2 * (sets_.size() + msets_.size());
+            L.step = cnt;
+            L.done = cnt + 1;
+            L.n_shots = (int)(j - i);
+            L.n_groups = n_groups;
+            L.total_items = items;
+            S.grid = items + rec;
+            if (int rc = raise_smem_limit(batch_march_kernel_any(S.M), march_smem_bytes_any(S.M))) return rc;
+            msets_.push_back(S);
+            i = j;
+        }
+        if (!msets_.empty()) {
+            const int n = (int)msets_.size();
+            fomo::march_counters_kernel<<<(n + 255) / 256, 256, 0, st_>>>(d_counters_ + 2 * sets_.size(), n,
+                                                                         (int)(k_host_ + 1));
+            CUDA_TRY(cudaGetLastError());
+        }
         return FOMO_OK;
     }
 
@@ -774,13 +940,15 @@ class Server {
     }
 
     // ------------------------------------------------------------ stepping
-    int launches_per_step() const { return 4 * (int)sets_.size(); }
+    int launches_per_step() const { return 4 * (int)sets_.size() + (int)msets_.size(); }
 
     // One batch step, set after set.  `after_band`: the last launch on the
     // stream is the previous step's last stress band pass, so the first
     // velocity launch may start beside it (every later tile launch follows
     // a band pass).
     void enqueue_step(bool after_band) {
+        // the previous step ended with a band pass only without fused-step sets
+        after_band = after_band && msets_.empty();
         for (size_t i = 0; i < sets_.size(); ++i) {
             const LaunchSet& S = sets_[i];
             launch_batch(true, S, st_, after_band || i > 0);
@@ -788,6 +956,18 @@ class Server {
             launch_batch(false, S, st_, true);
             fomo::batch_band_kernel<false, fomo::BatchStrLaunch><<<S.grid_b, 32, 0, st_>>>(*S.ls);
         }
+        for (const MarchSet& S : msets_) {
+            const cudaError_t e = batch_march_launch_any(S.M, S.grid, st_, *S.L);
+            if (e != cudaSuccess && enqueue_err_ == cudaSuccess) enqueue_err_ = e;
+        }
+    }
+
+    // The first launch error of the fused-step sets since the last check.
+    int take_enqueue_error() {
+        const cudaError_t e = enqueue_err_;
+        enqueue_err_ = cudaSuccess;
+        if (e != cudaSuccess) return fail(FOMO_ECUDA, "fused-step batch launch failed: %s", cudaGetErrorString(e));
+        return FOMO_OK;
     }
 
     int graph_for(int K, cudaGraphExec_t* out) {
@@ -800,6 +980,10 @@ class Server {
         CUDA_TRY(cudaStreamBeginCapture(st_, cudaStreamCaptureModeThreadLocal));
         for (int k = 0; k < K; ++k) enqueue_step(k > 0);
         cudaError_t e = cudaStreamEndCapture(st_, &g);
+        if (int rc = take_enqueue_error()) {
+            if (g) cudaGraphDestroy(g);
+            return rc;
+        }
         if (e != cudaSuccess) return fail(FOMO_ECUDA, "graph capture failed: %s", cudaGetErrorString(e));
         cudaGraphExec_t x = nullptr;
         e = cudaGraphInstantiate(&x, g, 0);
@@ -915,6 +1099,7 @@ class Server {
             for (int k = 0; k < n; ++k) enqueue_step(k > 0);
             nvtxRangePop();
             CUDA_TRY(cudaGetLastError());
+            if (int rc = take_enqueue_error()) return rc;
         }
         if (measure) {
             CUDA_TRY(cudaEventRecord(ms.b, st_));

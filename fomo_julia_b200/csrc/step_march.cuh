@@ -219,22 +219,61 @@ __device__ __forceinline__ void march_band_rows(const StepParams& P, const float
     }
 }
 
+// The descriptors one item uses: its shot's tau boxes and, when the item
+// prefetches, the L2-prefetch boxes (pf == false: none are read).
+struct MarchMapRefs {
+    const CUtensorMap *xx, *zz, *xz;
+    const CUtensorMap *vx, *vz, *b0, *b1, *b2, *b3, *lam, *mu, *mxz;
+    bool pf;
+};
+__device__ __forceinline__ MarchMapRefs refs_of(const MarchMaps& m) {
+    return {&m.xx, &m.zz, &m.xz, &m.vx, &m.vz, &m.b0, &m.b1, &m.b2, &m.b3, &m.lam, &m.mu, &m.mxz, true};
+}
+
+// Item `item` of a shot's fused step: bottom segments first (they march the
+// band), and within a segment the two edge strips first (they apply the side
+// rules).
+__device__ __forceinline__ void march_item_of(const MarchArgs& A, int item, int* strip, int* seg) {
+    *seg = A.n_segs - 1 - item / A.n_strips;
+    const int k = item % A.n_strips;
+    *strip = k == 0 ? 0 : (k == 1 ? A.n_strips - 1 : k - 1);
+}
+
+// Thread 0: TMA loads of the tau boxes of iteration t into stage slot
+// t % kMStages, and (mp.pf) L2 prefetches of the pointwise operands' boxes.
 template <int M>
-__global__ void __launch_bounds__(kMThreads, 2)
-    march_kernel(const __grid_constant__ StepParams P, const __grid_constant__ MarchArgs A,
-                 const __grid_constant__ MarchMaps mp) {
+__device__ __forceinline__ void march_issue(const MarchArgs& A, const MarchMapRefs& mp, float* stage, uint64_t* full,
+                                            int x0, int za, int t) {
+    using G = MGeo<M>;
+    const int s = t % kMStages;
+    float* dst = stage + s * G::STAGE;
+    const int vr0 = za - M + t * kMR, xa = x0 - G::HV;
+    mbar_expect_tx(full + s, 3 * G::TW * G::TH * 4);  // the bytes of the three boxes
+    tma_load_2d(dst, mp.xx, x0 - 2 * G::HV, vr0 - M, full + s);
+    tma_load_2d(dst + G::TAU, mp.zz, x0 - 2 * G::HV, vr0 - M, full + s);
+    tma_load_2d(dst + 2 * G::TAU, mp.xz, x0 - 2 * G::HV, vr0 - M, full + s);
+    if (mp.pf) {
+        tma_prefetch_2d(mp.vx, xa, vr0);
+        tma_prefetch_2d(mp.vz, xa, vr0);
+        tma_prefetch_2d(mp.b0, xa, vr0);
+        tma_prefetch_2d(mp.b2, xa, vr0);
+        if (!A.iso) {
+            tma_prefetch_2d(mp.b1, xa, vr0);
+            tma_prefetch_2d(mp.b3, xa, vr0);
+        }
+        tma_prefetch_2d(mp.lam, x0, vr0 + M);
+        tma_prefetch_2d(mp.mu, x0, vr0 + M);
+        tma_prefetch_2d(mp.mxz, x0, vr0 + M);
+    }
+}
+
+// One (strip, segment) of a shot's time step; src_w is the wavelet sample
+// added to txx and tzz at the source cell this step.
+template <int M>
+__device__ __forceinline__ void march_item(const StepParams& P, const MarchArgs& A, const MarchMapRefs& mp,
+                                           int strip, int seg, float src_w) {
     using G = MGeo<M>;
     extern __shared__ __align__(128) float smem[];
-    const int bid = blockIdx.x;
-    if (bid >= A.n_items) {
-        record_block(P, bid - A.n_items, P.rec_k);
-        return;
-    }
-    // Items: bottom segments first (they march the band), and within a
-    // segment the two edge strips first (they apply the side rules).
-    const int seg = A.n_segs - 1 - bid / A.n_strips;
-    const int k = bid % A.n_strips;
-    const int strip = k == 0 ? 0 : (k == 1 ? A.n_strips - 1 : k - 1);
     const bool last_strip = strip == A.n_strips - 1;
     const int x0 = last_strip ? A.x_last : strip * G::W;
     const int x_end = last_strip ? min(x0 + G::W, (P.nx + 3) / 4 * 4) : min(x0 + G::W, A.x_last);
@@ -251,30 +290,10 @@ __global__ void __launch_bounds__(kMThreads, 2)
     float* s_last = ring + 2 * G::RING;                // [3][64] stress finals of a block's last row
     uint64_t* full = reinterpret_cast<uint64_t*>(s_last + 3 * kMVW);
 
-    auto issue = [&](int t) {
-        const int s = t % kMStages;
-        float* dst = stage + s * G::STAGE;
-        const int vr0 = za - M + t * kMR;
-        mbar_expect_tx(full + s, 3 * G::TW * G::TH * 4);  // the bytes of the three boxes
-        tma_load_2d(dst, &mp.xx, x0 - 2 * G::HV, vr0 - M, full + s);
-        tma_load_2d(dst + G::TAU, &mp.zz, x0 - 2 * G::HV, vr0 - M, full + s);
-        tma_load_2d(dst + 2 * G::TAU, &mp.xz, x0 - 2 * G::HV, vr0 - M, full + s);
-        tma_prefetch_2d(&mp.vx, xa, vr0);
-        tma_prefetch_2d(&mp.vz, xa, vr0);
-        tma_prefetch_2d(&mp.b0, xa, vr0);
-        tma_prefetch_2d(&mp.b2, xa, vr0);
-        if (!A.iso) {
-            tma_prefetch_2d(&mp.b1, xa, vr0);
-            tma_prefetch_2d(&mp.b3, xa, vr0);
-        }
-        tma_prefetch_2d(&mp.lam, x0, vr0 + M);
-        tma_prefetch_2d(&mp.mu, x0, vr0 + M);
-        tma_prefetch_2d(&mp.mxz, x0, vr0 + M);
-    };
     if (threadIdx.x == 0) {
         for (int s = 0; s < kMStages; ++s) mbar_init(full + s, 1);
         fence_barrier_init();
-        for (int t = 0; t < min(kMStages, n_it); ++t) issue(t);
+        for (int t = 0; t < min(kMStages, n_it); ++t) march_issue<M>(A, mp, stage, full, x0, za, t);
     }
     __syncthreads();
 
@@ -298,8 +317,8 @@ __global__ void __launch_bounds__(kMThreads, 2)
             const int si = P.src_i - (x0 - 2 * G::HV), sj = P.src_j - (vr0 - M);
             if (si >= 0 && si < G::TW && sj >= 0 && sj < G::TH) {  // block-uniform
                 if (threadIdx.x == 0) {
-                    tau[sj * G::TW + si] = fadd(tau[sj * G::TW + si], P.src_w);
-                    tau[G::TAU + sj * G::TW + si] = fadd(tau[G::TAU + sj * G::TW + si], P.src_w);
+                    tau[sj * G::TW + si] = fadd(tau[sj * G::TW + si], src_w);
+                    tau[G::TAU + sj * G::TW + si] = fadd(tau[G::TAU + sj * G::TW + si], src_w);
                 }
                 __syncthreads();
             }
@@ -389,7 +408,7 @@ __global__ void __launch_bounds__(kMThreads, 2)
         __syncthreads();  // velocity block t in the ring; every thread is done with iteration t-1
         if (threadIdx.x == 0 && t >= 2 && t + 2 < n_it) {
             fence_proxy_async_smem();  // generic accesses of the slot before the TMA overwrites it
-            issue(t + 2);
+            march_issue<M>(A, mp, stage, full, x0, za, t + 2);
         }
         // ------------------------------------------------ stress block t-1
         if (t >= 1) {
@@ -499,6 +518,124 @@ __global__ void __launch_bounds__(kMThreads, 2)
                 stg4(P.out[TXZ] + cell(P, xs, j), oxz);
             }
         }
+    }
+}
+
+// The fused step of one shot: items (strip, segment) first, then the blocks
+// that record the receivers of step P.rec_k.
+template <int M>
+__global__ void __launch_bounds__(kMThreads, 2)
+    march_kernel(const __grid_constant__ StepParams P, const __grid_constant__ MarchArgs A,
+                 const __grid_constant__ MarchMaps mp) {
+    const int bid = blockIdx.x;
+    if (bid >= A.n_items) {
+        record_block(P, bid - A.n_items, P.rec_k);
+        return;
+    }
+    int strip, seg;
+    march_item_of(A, bid, &strip, &seg);
+    march_item<M>(P, A, refs_of(mp), strip, seg, P.src_w);
+}
+
+// ---------------------------------------------------------------- many shots per launch
+// The batched fused step: one launch per batch step covers up to
+// kMarchShots shots, grouped by medium (and HABC width: one layout per
+// group).  Inside a group the shots' items are interleaved item-major
+// (block = item * n + shot), so the shots' copies of one (strip, segment) run
+// side by side and the medium's rows come from HBM once and from L2 for the
+// others.  The batch step comes from a device counter, so every launch of a
+// batch has the same parameters and a run of K steps can be captured once
+// into a CUDA graph: each block reads the counter first, and the last block to
+// finish advances it for the next launch.  Blocks of shots outside their step
+// range return at once; the receiver blocks record step ks-1 of each shot,
+// including the shot's last step one batch step later, exactly like the
+// split batch launches.
+constexpr int kMarchShots = 12;
+constexpr int kMarchGroups = 8;
+
+struct MarchShot {
+    StepParams P[2];        // the step reads copy c (P[c].in) and writes copy 1-c (P[c].out), all five fields
+    const float* wavelet;
+    int n_wavelet;
+    int start;              // batch step of the shot's step 1 (>= 1)
+    int nt;
+    int pad_;
+};
+
+struct MarchGroup {
+    MarchArgs A;            // the group's layout, buoyancy and status word
+    int first, n;           // shots first .. first+n-1
+    int item_off;           // the group's first block
+    int pad_;
+};
+
+struct BatchMarchLaunch {
+    int* step;              // batch step (1-based) of this launch
+    int* done;              // blocks of this launch finished so far
+    int n_shots, n_groups, total_items, pad_;
+    int rec_off[kMarchShots + 1];  // first receiver block of each shot (after the items)
+    MarchGroup groups[kMarchGroups];
+    MarchShot shot[kMarchShots];
+    CUtensorMap tau[kMarchShots][2][3];  // tau boxes (TW x TH) of copy c
+};
+
+static_assert(sizeof(BatchMarchLaunch) <= 32764, "kernel parameters above the 32764-byte limit");
+
+template <int M>
+__device__ __forceinline__ void batch_march_block(const BatchMarchLaunch& L, int step) {
+    const int bid = blockIdx.x;
+    if (bid < L.total_items) {
+        int g = 0;
+#pragma unroll 1
+        for (int h = 1; h < L.n_groups; ++h)
+            if (L.groups[h].item_off <= bid) g = h;
+        const MarchGroup& G = L.groups[g];
+        const int r = bid - G.item_off;
+        const int s = G.first + r % G.n, item = r / G.n;
+        const MarchShot& S = L.shot[s];
+        const int ks = step - S.start + 1;
+        if (ks < 1 || ks > S.nt) return;
+        const int a = (ks - 1) & 1;
+        int strip, seg;
+        march_item_of(G.A, item, &strip, &seg);
+        const MarchMapRefs mp{&L.tau[s][a][0], &L.tau[s][a][1], &L.tau[s][a][2], nullptr, nullptr, nullptr,
+                              nullptr,        nullptr,        nullptr,        nullptr, nullptr, nullptr, false};
+        const float src_w = ks <= S.n_wavelet ? __ldg(S.wavelet + ks - 1) : 0.f;
+        march_item<M>(S.P[a], G.A, mp, strip, seg, src_w);
+        return;
+    }
+    const int rb = bid - L.total_items;
+    if (rb >= L.rec_off[L.n_shots]) return;
+    int s = 0;
+#pragma unroll 1
+    while (L.rec_off[s + 1] <= rb) ++s;
+    const MarchShot& S = L.shot[s];
+    const int ks = step - S.start + 1;
+    if (ks >= 2 && ks <= S.nt + 1) record_block(S.P[(ks - 1) & 1], rb - L.rec_off[s], ks - 1);  // copy (ks-1)&1
+}
+
+template <int M>
+__global__ void __launch_bounds__(kMThreads, 2) batch_march_kernel(const __grid_constant__ BatchMarchLaunch L) {
+    const int step = *reinterpret_cast<volatile const int*>(L.step);
+    batch_march_block<M>(L, step);
+    __syncthreads();
+    if (threadIdx.x == 0) {  // every block has read the step once the last one gets here
+        __threadfence();
+        if (atomicAdd(L.done, 1) == (int)gridDim.x - 1) {
+            *L.done = 0;
+            *reinterpret_cast<volatile int*>(L.step) = step + 1;
+            __threadfence();
+        }
+    }
+}
+
+// Counters of n batched fused-step sets at a table rebuild: step of set i
+// (counters[2i]) = `step`, its finished-block count (counters[2i+1]) = 0.
+static __global__ void march_counters_kernel(int* counters, int n, int step) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) {
+        counters[2 * i] = step;
+        counters[2 * i + 1] = 0;
     }
 }
 

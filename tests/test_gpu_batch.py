@@ -63,7 +63,15 @@ def source_xs(c: Case, n):
 MEDIUM_A = dict(nx_in=231, nz_in=90, seed=13, nbc=10, fd_order=8, nt=100, n_rec=41)
 
 
-def test_batch_equals_single_shots_and_oracle(b200, oracle_lib):
+@pytest.fixture(params=["auto", "split"])
+def step_mode(request):
+    """Fused-step launches ("auto" on this medium) and the split launches."""
+    F.set_step_kernel(request.param)
+    yield request.param
+    F.set_step_kernel("auto")
+
+
+def test_batch_equals_single_shots_and_oracle(b200, oracle_lib, step_mode):
     c = layered(**MEDIUM_A)
     S = setup(c, b200)
     xs = source_xs(c, 6)
@@ -71,6 +79,9 @@ def test_batch_equals_single_shots_and_oracle(b200, oracle_lib):
     res = F.run_shots(b200, None, S.med, S.H, S.a, S.rec, cfg, params_of(S), batched=True)
     assert len(res) == len(xs)
     assert res[0].stats["steps"] == len(xs) * c.nt
+    # one fused launch per batch step, or four split launches (tiles and band passes of both half steps)
+    per_step = res[0].stats["kernel_launches"] / c.nt
+    assert (per_step < 2.5) == (step_mode == "auto"), per_step
     for k, r in enumerate(res):
         src = F.create_source(S.med, cfg.shots[k], cfg.wavelet)
         assert (r.src_i, r.src_j) == (src.i, src.j)

@@ -50,12 +50,21 @@ def assert_same(g_gpu, g_orc, f_gpu, f_orc, exact=True):
     for f in FIELDS:
         num = np.linalg.norm((f_gpu[f] - f_orc[f]).astype(np.float64))
         den = max(np.linalg.norm(f_orc[f].astype(np.float64)), 1e-30)
-        assert num / den <= TOL, f"field {f}: rel L2 {num / den:.3e}"
+        assert num / den <= TOL, f"field {f}: rel L2 {num / den:.3e} ({mismatch(f_gpu[f], f_orc[f])})"
     if exact:
         diff = np.abs(g_gpu - g_orc).max() if g_gpu.size else 0.0
         assert np.array_equal(g_gpu, g_orc), f"gather not bit-identical (max abs diff {diff:.3e})"
         for f in FIELDS:
-            assert np.array_equal(f_gpu[f], f_orc[f]), f"field {f} not bit-identical"
+            assert np.array_equal(f_gpu[f], f_orc[f]), f"field {f} not bit-identical: {mismatch(f_gpu[f], f_orc[f])}"
+
+
+def mismatch(a, b) -> str:
+    """Where two (nx, nz) fields differ (0-based cell indices)."""
+    ii, jj = np.nonzero(a != b)
+    if ii.size == 0:
+        return "no difference"
+    return (f"{ii.size} cells, i {ii.min()}..{ii.max()}, j {jj.min()}..{jj.max()}, "
+            f"max abs {np.abs(a.astype(np.float64) - b).max():.3e}")
 
 
 def _anisotropic_grid_case():

@@ -50,7 +50,10 @@ def parse():
     p.add_argument("--no-batched", action="store_true", help="skip the batched-shots section")
     p.add_argument("--no-serving", action="store_true", help="skip the serving section")
     p.add_argument("--batch-nt", type=int, default=None, help="override nt of the batched section (development)")
-    p.add_argument("--serve-requests", type=int, default=48)
+    p.add_argument("--serve-requests", type=int, default=48,
+                   help="requests of the serving sample (the full stream of the serving workload is 2000)")
+    p.add_argument("--serve-load", type=float, default=4.0,
+                   help="offered load of the serving sample, as a multiple of the sequential plain capacity")
     p.add_argument("--no-uneven", action="store_true", help="skip the uneven-batch section")
     p.add_argument("--step-kernel", choices=["auto", "split", "fused"], default="auto",
                    help="single-shot time-step kernels: the fused step where it applies (auto), or one of the two")
@@ -408,7 +411,7 @@ def serving_section(args, c1):
     n = args.serve_requests
     probe = synthetic.serving_requests(n, nx_in, dxs, 1.0)
     plain_total = sum(plain_step[q.medium] * q.nt for q in probe)
-    rate = 4.0 * n / plain_total  # offered load: four times what sequential plain shots sustain
+    rate = args.serve_load * n / plain_total  # offered load: a multiple of what sequential plain shots sustain
     reqs = synthetic.serving_requests(n, nx_in, dxs, rate)
     budget = 150 << 30
     try:
@@ -448,9 +451,14 @@ def serving_section(args, c1):
     from fomo_julia_b200.serving import percentile
     return {
         "requests": n, "media": [[m.nx, m.nz] for m in M], "arrival_rate_per_s": rate,
-        "arrival": "Poisson, rate = 4 x the sequential plain capacity of this request mix",
+        "arrival": f"Poisson, rate = {args.serve_load:g} x the sequential plain capacity of this request mix",
+        "offered_load_vs_plain_capacity": args.serve_load,
+        "fraction_of_full_stream": n / 2000.0,
         "hbm_budget_bytes": budget, "makespan_s": makespan,
         "p50_latency_ms": percentile(lat, 50), "p99_latency_ms": percentile(lat, 99),
+        "p50_run_ms": percentile([r.stats["run_ms"] for r in results], 50),
+        "p99_run_ms": percentile([r.stats["run_ms"] for r in results], 99),
+        "latency_note": "latency = submit to gather on the host; run = admission to completion (queueing excluded)",
         "served_shots_per_hour": n * 3600.0 / makespan,
         "plain_shots_per_hour": n * 3600.0 / plain_total,
         "speedup_vs_plain": plain_total / makespan,

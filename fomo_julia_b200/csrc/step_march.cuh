@@ -167,6 +167,8 @@ struct SmemRows {
     }
 };
 
+constexpr int kMarchWarps = 6;  // warps that run the band recurrence (fields x 28-column strips)
+
 // The bottom-band recurrence (rows nz-nbc-1 .. nz-2) of one field over the
 // band rows [ja, jb) of one block: `pre` holds the block's values after the
 // stencil update (band rows) and final values (rows above), and receives the
@@ -199,8 +201,18 @@ __device__ __forceinline__ void march_band_rows(const StepParams& P, const float
     float ovp = have ? __ldg(oin + cell(P, i, ja - 1)) : 0.f;
     const bool store = have && lane >= 2 && lane < 30;
     const bool own = store && i >= own_lo && i < own_hi;
-    for (int j = ja; j < jb; ++j) {
-        const float pv = have ? *at(j) : 0.f;
+    // Every lane reads its column's values of the block's band rows before any
+    // warp writes a final back: the margin lanes read columns that the
+    // neighbouring warp stores.
+    float pvs[kMR];
+#pragma unroll
+    for (int r = 0; r < kMR; ++r) pvs[r] = (have && ja + r < jb) ? *at(ja + r) : 0.f;
+    asm volatile("bar.sync 1, %0;" ::"n"(kMarchWarps * 32) : "memory");
+#pragma unroll
+    for (int r = 0; r < kMR; ++r) {
+        const int j = ja + r;
+        if (j >= jb) break;
+        const float pv = pvs[r];
         const float ov = have ? __ldg(oin + cell(P, i, j)) : 0.f;
         const float w = __ldg(tab + min(min(dxi, nz - 1 - j), b + 1));
         const float pv_nb = __shfl_sync(FULL, pv, nb);
@@ -386,7 +398,7 @@ __device__ __forceinline__ void march_item(const StepParams& P, const MarchArgs&
                 *reinterpret_cast<float4*>(rvz) = oz;
                 if (band_rows) {
                     __syncthreads();
-                    if (warp < 6) {
+                    if (warp < kMarchWarps) {  // all kMarchWarps warps take the march's named barrier
                         const int f = warp / 3, ws = warp % 3;
                         march_band_rows(P, w_table(P, f), in_field(P, VX + f), out_field(P, VX + f),
                                         ring + f * G::RING, kMVW, xa, vr0, (t % kMRing) * kMR, G::RING_ROWS, xa,
@@ -488,7 +500,7 @@ __device__ __forceinline__ void march_item(const StepParams& P, const MarchArgs&
                 if (band_rows) {
                     const int ja = max(sr0, j0), jb = min(min(sr0 + kMR, nz - 1), zb);
                     __syncthreads();
-                    if (warp < 6) {
+                    if (warp < kMarchWarps) {  // all kMarchWarps warps take the march's named barrier
                         const int f = warp / 2, ws = warp % 2;
                         // the row above the first band row: in this block, or the previous block's last row
                         march_band_rows(P, P.w_tab[2], in_field(P, TXX + f), out_field(P, TXX + f),

@@ -134,7 +134,7 @@ struct Context {
     int device = -1;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-    int* d_status = nullptr;   // device error word of the kernels
+    int* d_status = nullptr;   // device error word of the kernels, then the fused step's work queue (2 ints)
     cudaMemPool_t pool = nullptr;
     uint64_t next = 1;
     std::unordered_map<uint64_t, std::unique_ptr<Object>> objs;
@@ -541,7 +541,9 @@ int run_steps_march(Shot& s, Medium& m, Wavefield& w, int n_steps, Profile* prof
     buoyancy_ptrs(m, A.b);
     A.iso = iso ? 1 : 0;
     A.status = C.d_status;
+    A.queue = C.d_status + 2;  // zero between launches: the last block to leave resets it
     const int rec_blocks = (s.n_rec + fomo::kMThreads - 1) / fomo::kMThreads;
+    const int slots = march_slots<M>();
     CUDA_TRY(cudaEventRecord(C.ev0, C.stream));
     const int k_begin = s.k_done + 1, k_end = std::min(s.nt, s.k_done + n_steps);
     nvtxRangePushA("fomo_b200 time loop (fused step)");
@@ -569,7 +571,9 @@ int run_steps_march(Shot& s, Medium& m, Wavefield& w, int n_steps, Profile* prof
         mp.mu = m.mod_maps[1];
         mp.mxz = m.mod_maps[2];
         if (prof && prof->add(C.stream, 4)) return fail(FOMO_ECUDA, "profiling event failed");
-        CUDA_TRY(fomo::march_launch<M>(A.n_items + (P.rec_k ? rec_blocks : 0), C.stream, P, A, mp));
+        A.n_rec_items = P.rec_k ? rec_blocks : 0;
+        // persistent blocks: as many as are resident at once, at most one per item
+        CUDA_TRY(fomo::march_launch<M>(std::min(A.n_items + A.n_rec_items, slots), C.stream, P, A, mp));
         if (prof && prof->end(C.stream)) return fail(FOMO_ECUDA, "profiling event failed");
         s.launches += 1;
         w.cur = b;
@@ -759,8 +763,8 @@ int fomo_b200_init(int device) {
     CUDA_TRY(cudaStreamCreateWithFlags(&C.stream, cudaStreamNonBlocking));
     CUDA_TRY(cudaEventCreate(&C.ev0));
     CUDA_TRY(cudaEventCreate(&C.ev1));
-    CUDA_TRY(cudaMalloc(&C.d_status, sizeof(int)));
-    CUDA_TRY(cudaMemset(C.d_status, 0, sizeof(int)));
+    CUDA_TRY(cudaMalloc(&C.d_status, 4 * sizeof(int)));
+    CUDA_TRY(cudaMemset(C.d_status, 0, 4 * sizeof(int)));
     cudaMemPoolProps props;
     std::memset(&props, 0, sizeof(props));
     props.allocType = cudaMemAllocationTypePinned;

@@ -329,7 +329,7 @@ class Server {
         CUDA_TRY(cudaMemPoolCreate(&pool_, &props));
         uint64_t keep = UINT64_MAX;
         CUDA_TRY(cudaMemPoolSetAttribute(pool_, cudaMemPoolAttrReleaseThreshold, &keep));
-        CUDA_TRY(cudaMalloc(&d_ctl_, 256 + 2 * sizeof(int) * kMaxInFlight));
+        CUDA_TRY(cudaMalloc(&d_ctl_, 256 + 4 * sizeof(int) * kMaxInFlight));
         d_status_ = reinterpret_cast<int*>(d_ctl_ + 128);
         d_counters_ = reinterpret_cast<int*>(d_ctl_ + 256);
         CUDA_TRY(cudaMemset(d_status_, 0, sizeof(int)));
@@ -906,13 +906,14 @@ class Server {
                 for (int c = 0; c < 2; ++c)
                     for (int f = 0; f < 3; ++f) L.tau[t][c][f] = r.halo[c][fomo::TXX + f];
             }
-            int* cnt = d_counters_ + 2 * (sets_.size() + msets_.size());
+            // counters after the split sets' (2 ints each): step, blocks left, next item, spare
+            int* cnt = d_counters_ + 2 * sets_.size() + 4 * msets_.size();
             L.step = cnt;
-            L.done = cnt + 1;
             L.n_shots = (int)(j - i);
             L.n_groups = n_groups;
             L.total_items = items;
-            S.grid = items + rec;
+            L.n_rec_items = rec;
+            S.grid = std::min(items + rec, march_slots_of(S.M));  // persistent blocks
             if (int rc = raise_smem_limit(batch_march_kernel_any(S.M), march_smem_bytes_any(S.M))) return rc;
             msets_.push_back(S);
             i = j;

@@ -69,6 +69,8 @@ struct MarchArgs {
     const float* b[4];     // buoyancy dtx/rho_vx, dtz/rho_vx, dtx/rho_vz, dtz/rho_vz
     int iso;
     int* status;
+    int* queue;            // [0] next item, [1] blocks that left (both zero between launches)
+    int n_rec_items;       // receiver items after the strip-segment items
     int n_strips, n_segs, n_items;
     int x_last;            // first output column of the last (right-aligned) strip
     int seg_z[kMMaxSegs + 1];  // segment s: stress rows [seg_z[s], seg_z[s+1])
@@ -251,13 +253,14 @@ __device__ __forceinline__ void march_item_of(const MarchArgs& A, int item, int*
     *strip = k == 0 ? 0 : (k == 1 ? A.n_strips - 1 : k - 1);
 }
 
-// Thread 0: TMA loads of the tau boxes of iteration t into stage slot
-// t % kMStages, and (mp.pf) L2 prefetches of the pointwise operands' boxes.
+// Thread 0: TMA loads of the tau boxes of iteration t (the block's stage
+// number g: slot g % kMStages) and, with mp.pf, L2 prefetches of the
+// pointwise operands' boxes.
 template <int M>
 __device__ __forceinline__ void march_issue(const MarchArgs& A, const MarchMapRefs& mp, float* stage, uint64_t* full,
-                                            int x0, int za, int t) {
+                                            int x0, int za, int t, int g) {
     using G = MGeo<M>;
-    const int s = t % kMStages;
+    const int s = g % kMStages;
     float* dst = stage + s * G::STAGE;
     const int vr0 = za - M + t * kMR, xa = x0 - G::HV;
     mbar_expect_tx(full + s, 3 * G::TW * G::TH * 4);  // the bytes of the three boxes
@@ -279,11 +282,22 @@ __device__ __forceinline__ void march_issue(const MarchArgs& A, const MarchMapRe
     }
 }
 
-// One (strip, segment) of a shot's time step; src_w is the wavelet sample
-// added to txx and tzz at the source cell this step.
+// Rows of a segment's velocity block t that its stress reads (the last
+// block feeds only 2M stress rows): [vr0, march_v_hi).
 template <int M>
-__device__ __forceinline__ void march_item(const StepParams& P, const MarchArgs& A, const MarchMapRefs& mp,
-                                           int strip, int seg, float src_w) {
+__device__ __forceinline__ int march_v_hi(int vr0, int t, int n_it, int zb) {
+    return min(vr0 + (t < n_it - 1 ? kMR : 2 * M), zb + M);
+}
+
+// One (strip, segment) of a shot's time step; src_w is the wavelet sample
+// added to txx and tzz at the source cell this step.  g is the block's
+// running stage number (stage slots and mbarrier phases continue across the
+// items a block runs); it advances by the item's iterations.  The caller
+// has synchronised the block since its previous item.  Returns false (all
+// threads alike) if a TMA load did not land: the status word holds the error.
+template <int M>
+__device__ __forceinline__ bool march_item(const StepParams& P, const MarchArgs& A, const MarchMapRefs& mp,
+                                           int strip, int seg, float src_w, int& g, int* s_err) {
     using G = MGeo<M>;
     extern __shared__ __align__(128) float smem[];
     const bool last_strip = strip == A.n_strips - 1;
@@ -296,18 +310,13 @@ __device__ __forceinline__ void march_item(const StepParams& P, const MarchArgs&
     const int j0 = nz - b - 1;                        // first bottom-band row
     const int edge = max(b + 2, M);
     const bool side = xa < edge || xa + kMVW > nx - edge;  // block-uniform: side HABC or rim columns
+    const int g0 = g;
+    g += n_it;
 
     float* stage = smem;
     float* ring = smem + kMStages * G::STAGE;          // [2 fields][48 rows][64]
     float* s_last = ring + 2 * G::RING;                // [3][64] stress finals of a block's last row
     uint64_t* full = reinterpret_cast<uint64_t*>(s_last + 3 * kMVW);
-
-    if (threadIdx.x == 0) {
-        for (int s = 0; s < kMStages; ++s) mbar_init(full + s, 1);
-        fence_barrier_init();
-        for (int t = 0; t < min(kMStages, n_it); ++t) march_issue<M>(A, mp, stage, full, x0, za, t);
-    }
-    __syncthreads();
 
     const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
     const int xv = xa + 4 * tx;          // first column of the thread's velocity cells
@@ -319,11 +328,45 @@ __device__ __forceinline__ void march_item(const StepParams& P, const MarchArgs&
     const bool s_in = s_col && xs < nx;
     const int warp = threadIdx.x >> 5;
 
+    if (threadIdx.x == 0) {
+        fence_proxy_async_smem();  // the previous item's generic accesses of the slots before the TMA refills them
+        for (int t = 0; t < min(kMStages, n_it); ++t) march_issue<M>(A, mp, stage, full, x0, za, t, g0 + t);
+        *s_err = mbar_wait_parity(full + g0 % kMStages, (g0 / kMStages) & 1, A.status) ? 0 : 1;
+    }
+    // Pointwise operands of velocity block t, loaded one phase before they are used.
+    float4 pvx = make_float4(0.f, 0.f, 0.f, 0.f), pvz = pvx, pb0 = pvx, pb1 = pvx, pb2 = pvx, pb3 = pvx;
+    auto load_v = [&](int t) {
+        const int j = za - M + t * kMR + ty;
+        if (v_in && j >= 0 && j < nz && j < march_v_hi<M>(za - M + t * kMR, t, n_it, zb)) {
+            const size_t c = cell(P, xv, j);
+            pvx = ldg4(P.in[VX] + c);
+            pvz = ldg4(P.in[VZ] + c);
+            pb0 = ldg4(A.b[0] + c);
+            pb2 = ldg4(A.b[2] + c);
+            pb1 = A.iso ? pb0 : ldg4(A.b[1] + c);
+            pb3 = A.iso ? pb2 : ldg4(A.b[3] + c);
+        }
+    };
+    load_v(0);
+    __syncthreads();
+    if (*s_err) return false;
+
     for (int t = 0; t < n_it; ++t) {
-        const int s = t % kMStages;
-        float* tau = stage + s * G::STAGE;
-        if (!mbar_wait_parity(full + s, (t / kMStages) & 1, A.status)) return;
+        const int gt = g0 + t;
+        float* tau = stage + (gt % kMStages) * G::STAGE;
         const int vr0 = za - M + t * kMR;
+        const int slot = t % kMRing;
+        // medium of stress block t-1, loaded now and used after the velocity
+        const int sr0 = za + (t - 1) * kMR;
+        const int js = sr0 + ty;
+        const bool s_row = t >= 1 && js < zb && js < nz;
+        float4 mlam = make_float4(0.f, 0.f, 0.f, 0.f), mmu = mlam, mmxz = mlam;
+        if (s_row && s_in) {
+            const size_t c = cell(P, xs, js);
+            mlam = ldg4(P.lam + c);
+            mmu = ldg4(P.mu_txx + c);
+            mmxz = ldg4(P.mu_txz + c);
+        }
         // ------------------------------------------------ the source, into this stage's copy
         {
             const int si = P.src_i - (x0 - 2 * G::HV), sj = P.src_j - (vr0 - M);
@@ -338,15 +381,10 @@ __device__ __forceinline__ void march_item(const StepParams& P, const MarchArgs&
         // ------------------------------------------------ velocity block t
         {
             const int j = vr0 + ty;
-            // rows the stress of this segment reads (the last block feeds 2M stress rows)
-            const int v_hi = min(vr0 + (t < n_it - 1 ? kMR : 2 * M), zb + M);
+            const int v_hi = march_v_hi<M>(vr0, t, n_it, zb);
             float4 ox = make_float4(0.f, 0.f, 0.f, 0.f), oz = ox;
             const bool row_ok = j < v_hi && j >= 0 && j < nz;
             if (row_ok && v_in) {
-                const size_t c = cell(P, xv, j);
-                const float4 vx = ldg4(P.in[VX] + c), vz = ldg4(P.in[VZ] + c);
-                const float4 b0 = ldg4(A.b[0] + c), b2 = ldg4(A.b[2] + c);
-                const float4 b1 = A.iso ? b0 : ldg4(A.b[1] + c), b3 = A.iso ? b2 : ldg4(A.b[3] + c);
                 const float* rxx = tau + (ty + M) * G::TW + 4 * tx;  // windows from column xv - 4
                 const float* rxz = tau + 2 * G::TAU + (ty + M) * G::TW + 4 * tx;
                 const float4 d1 = xderiv1<M, 0>(P, rxx);   // dtxx/dx: txx[i+l-1] - txx[i-l]
@@ -358,18 +396,18 @@ __device__ __forceinline__ void march_item(const StepParams& P, const MarchArgs&
 #pragma unroll
                 for (int q = 0; q < 2 * M; ++q) wz[q] = lds4(tau + G::TAU + (ty + 1 + q) * G::TW + 4 * tx + G::HV);
                 const float4 d4 = zderiv1<M>(P, wz);        // dtzz/dz: tzz[j+l] - tzz[j-l+1]
-                ox = add4(vx, add4(mul4(b0, d1), mul4(b1, d2)));
-                oz = add4(vz, add4(mul4(b2, d3), mul4(b3, d4)));
+                ox = add4(pvx, add4(mul4(pb0, d1), mul4(pb1, d2)));
+                oz = add4(pvz, add4(mul4(pb2, d3), mul4(pb3, d4)));
                 if (side || j < M || j > nz - 1 - M) {
 #pragma unroll
                     for (int c4 = 0; c4 < 4; ++c4)
                         if (!in_stencil(P, xv + c4, j)) {
-                            set_comp(ox, c4, comp(vx, c4));
-                            set_comp(oz, c4, comp(vz, c4));
+                            set_comp(ox, c4, comp(pvx, c4));
+                            set_comp(oz, c4, comp(pvz, c4));
                         }
                 }
             }
-            const int rr = (t % kMRing) * kMR + ty;    // ring row of grid row j
+            const int rr = slot * kMR + ty;    // ring row of grid row j
             float* rvx = ring + rr * kMVW + 4 * tx;
             float* rvz = ring + G::RING + rr * kMVW + 4 * tx;
             *reinterpret_cast<float4*>(rvx) = ox;
@@ -378,10 +416,10 @@ __device__ __forceinline__ void march_item(const StepParams& P, const MarchArgs&
             if (side || band_rows) {
                 __syncthreads();  // pre values of the block in the ring
                 if (side && row_ok && j >= b && j <= j0 - 1) {  // left/right HABC (free surface: rows nbc .. nz-nbc-2)
-                    const SmemRows pvx{ring, xa, vr0, (t % kMRing) * kMR, G::RING_ROWS, kMVW};
-                    const SmemRows pvz{ring + G::RING, xa, vr0, (t % kMRing) * kMR, G::RING_ROWS, kMVW};
-                    const HabcPoint<SmemRows> hx{P, pvx, P.in[VX], P.w_tab[0]};
-                    const HabcPoint<SmemRows> hz{P, pvz, P.in[VZ], P.w_tab[1]};
+                    const SmemRows pre_x{ring, xa, vr0, slot * kMR, G::RING_ROWS, kMVW};
+                    const SmemRows pre_z{ring + G::RING, xa, vr0, slot * kMR, G::RING_ROWS, kMVW};
+                    const HabcPoint<SmemRows> hx{P, pre_x, P.in[VX], P.w_tab[0]};
+                    const HabcPoint<SmemRows> hz{P, pre_z, P.in[VZ], P.w_tab[1]};
 #pragma unroll
                     for (int c4 = 0; c4 < 4; ++c4) {
                         const int i = xv + c4;
@@ -401,7 +439,7 @@ __device__ __forceinline__ void march_item(const StepParams& P, const MarchArgs&
                     if (warp < kMarchWarps) {  // all kMarchWarps warps take the march's named barrier
                         const int f = warp / 3, ws = warp % 3;
                         march_band_rows(P, w_table(P, f), in_field(P, VX + f), out_field(P, VX + f),
-                                        ring + f * G::RING, kMVW, xa, vr0, (t % kMRing) * kMR, G::RING_ROWS, xa,
+                                        ring + f * G::RING, kMVW, xa, vr0, slot * kMR, G::RING_ROWS, xa,
                                         xa + kMVW, x0, x_end, xa + 28 * ws, max(vr0, j0), min(v_hi, nz - 1),
                                         nullptr);
                     }
@@ -417,42 +455,50 @@ __device__ __forceinline__ void march_item(const StepParams& P, const MarchArgs&
                 stg4(P.out[VZ] + cell(P, xv, j), oz);
             }
         }
-        __syncthreads();  // velocity block t in the ring; every thread is done with iteration t-1
+        // velocity block t in the ring; every thread is done with iteration t-1.  Thread 0
+        // waits for the next iteration's tau boxes here, so the other threads sleep in the
+        // barrier instead of polling.
+        if (threadIdx.x == 0 && t + 1 < n_it)
+            *s_err = mbar_wait_parity(full + (gt + 1) % kMStages, ((gt + 1) / kMStages) & 1, A.status) ? 0 : 1;
+        __syncthreads();
+        if (*s_err) return false;
         if (threadIdx.x == 0 && t >= 2 && t + 2 < n_it) {
             fence_proxy_async_smem();  // generic accesses of the slot before the TMA overwrites it
-            march_issue<M>(A, mp, stage, full, x0, za, t + 2);
+            march_issue<M>(A, mp, stage, full, x0, za, t + 2, gt + 2);
         }
+        if (t + 1 < n_it) load_v(t + 1);  // velocity block t is done with the current ones
         // ------------------------------------------------ stress block t-1
         if (t >= 1) {
-            const int sr0 = za + (t - 1) * kMR;
-            const int j = sr0 + ty;
-            const float* told = stage + ((t - 1) % kMStages) * G::STAGE;  // stage t-1: rows from sr0 - 2M
-            const bool row_ok = j < zb && j < nz;
+            const int j = js;
+            const float* told = stage + ((gt - 1) % kMStages) * G::STAGE;  // stage t-1: rows from sr0 - 2M
+            const bool row_ok = s_row;
             float4 oxx = make_float4(0.f, 0.f, 0.f, 0.f), ozz = oxx, oxz = oxx;
             if (row_ok && s_in) {
-                const size_t c = cell(P, xs, j);
-                const float4 lam = ldg4(P.lam + c), mu = ldg4(P.mu_txx + c), mxz = ldg4(P.mu_txz + c);
                 const int bo = (ty + 2 * M) * G::TW + 2 * G::HV + 4 * tx;
                 const float4 txx = lds4(told + bo), tzz = lds4(told + G::TAU + bo);
                 const float4 txz = lds4(told + 2 * G::TAU + bo);
-                // ring row of grid row j - M is r (relative row (t-1)*16 + ty, modulo the ring)
+                // ring row of grid row j - M + q: r + q, wrapped once at the ring's end
                 const int r = ((t - 1) % kMRing) * kMR + ty;
                 const float* rvx = ring + 4 * tx;
                 const float* rvz = ring + G::RING + 4 * tx;
-                const float4 dxx = xderiv1<M, 1>(P, rvx + (r + M) % G::RING_ROWS * kMVW);  // vx[i+l] - vx[i-l+1]
-                const float4 dzx = xderiv1<M, 0>(P, rvz + (r + M) % G::RING_ROWS * kMVW);  // vz[i+l-1] - vz[i-l]
+                auto rrow = [&](int q) {
+                    const int x = r + q;
+                    return (x >= G::RING_ROWS ? x - G::RING_ROWS : x) * kMVW;
+                };
+                const float4 dxx = xderiv1<M, 1>(P, rvx + rrow(M));  // vx[i+l] - vx[i-l+1]
+                const float4 dzx = xderiv1<M, 0>(P, rvz + rrow(M));  // vz[i+l-1] - vz[i-l]
                 float4 wz[2 * M];
 #pragma unroll
-                for (int q = 0; q < 2 * M; ++q) wz[q] = lds4(rvz + (r + q) % G::RING_ROWS * kMVW + G::HV);
+                for (int q = 0; q < 2 * M; ++q) wz[q] = lds4(rvz + rrow(q) + G::HV);
                 const float4 dzz = zderiv1<M>(P, wz);       // vz[j+l-1] - vz[j-l]
 #pragma unroll
-                for (int q = 0; q < 2 * M; ++q) wz[q] = lds4(rvx + (r + 1 + q) % G::RING_ROWS * kMVW + G::HV);
+                for (int q = 0; q < 2 * M; ++q) wz[q] = lds4(rvx + rrow(q + 1) + G::HV);
                 const float4 dxz = zderiv1<M>(P, wz);       // vx[j+l] - vx[j-l+1]
-                const float4 l2m = add4(lam, mul4s(mu, 2.f));
+                const float4 l2m = add4(mlam, mul4s(mmu, 2.f));
                 const float4 ex = mul4s(dxx, P.dtx), ez = mul4s(dzz, P.dtz);
-                oxx = add4(txx, add4(mul4(l2m, ex), mul4(lam, ez)));
-                ozz = add4(tzz, add4(mul4(lam, ex), mul4(l2m, ez)));
-                oxz = add4(txz, mul4(mxz, add4(mul4s(dxz, P.dtz), mul4s(dzx, P.dtx))));
+                oxx = add4(txx, add4(mul4(l2m, ex), mul4(mlam, ez)));
+                ozz = add4(tzz, add4(mul4(mlam, ex), mul4(l2m, ez)));
+                oxz = add4(txz, mul4(mmxz, add4(mul4s(dxz, P.dtz), mul4s(dzx, P.dtx))));
                 if (side || j < M || j > nz - 1 - M) {
 #pragma unroll
                     for (int c4 = 0; c4 < 4; ++c4)
@@ -467,7 +513,7 @@ __device__ __forceinline__ void march_item(const StepParams& P, const MarchArgs&
             if (side || band_rows) {
                 // exchange through the slot of stage t-1 once every thread has read it
                 __syncthreads();
-                float* sp = stage + ((t - 1) % kMStages) * G::STAGE;  // [3][16][64], column 0 = x0
+                float* sp = stage + ((gt - 1) % kMStages) * G::STAGE;  // [3][16][64], column 0 = x0
                 if (s_col) {
                     *reinterpret_cast<float4*>(sp + ty * kMVW + 4 * tx) = oxx;
                     *reinterpret_cast<float4*>(sp + kMR * kMVW + ty * kMVW + 4 * tx) = ozz;
@@ -531,37 +577,63 @@ __device__ __forceinline__ void march_item(const StepParams& P, const MarchArgs&
             }
         }
     }
+    return true;
 }
 
-// The fused step of one shot: items (strip, segment) first, then the blocks
-// that record the receivers of step P.rec_k.
+// Work queue of a fused-step launch: a block takes items until none are
+// left; the last block to leave resets the queue for the next launch.
+__device__ __forceinline__ int march_next(int* queue, int* s_item) {
+    if (threadIdx.x == 0) *s_item = atomicAdd(queue, 1);
+    __syncthreads();
+    return *s_item;
+}
+__device__ __forceinline__ bool march_leave(int* queue) {  // true in thread 0 of the last block
+    if (threadIdx.x != 0) return false;
+    __threadfence();
+    if (atomicAdd(queue + 1, 1) != (int)gridDim.x - 1) return false;
+    queue[0] = 0;
+    queue[1] = 0;
+    __threadfence();
+    return true;
+}
+
+// The fused step of one shot: persistent blocks take items from the queue
+// A.queue -- the (strip, segment) items, then the receiver blocks of step
+// P.rec_k.
 template <int M>
 __global__ void __launch_bounds__(kMThreads, 2)
     march_kernel(const __grid_constant__ StepParams P, const __grid_constant__ MarchArgs A,
                  const __grid_constant__ MarchMaps mp) {
-    const int bid = blockIdx.x;
-    if (bid >= A.n_items) {
-        record_block(P, bid - A.n_items, P.rec_k);
-        return;
+    __shared__ int s_item, s_err;
+    int g = 0;
+    for (;;) {
+        const int item = march_next(A.queue, &s_item);
+        if (item >= A.n_items + A.n_rec_items) break;
+        if (item < A.n_items) {
+            int strip, seg;
+            march_item_of(A, item, &strip, &seg);
+            if (!march_item<M>(P, A, refs_of(mp), strip, seg, P.src_w, g, &s_err)) break;
+        } else {
+            record_block(P, item - A.n_items, P.rec_k);
+        }
+        __syncthreads();  // the block is done with the item's shared memory and s_item
     }
-    int strip, seg;
-    march_item_of(A, bid, &strip, &seg);
-    march_item<M>(P, A, refs_of(mp), strip, seg, P.src_w);
+    march_leave(A.queue);
 }
 
 // ---------------------------------------------------------------- many shots per launch
 // The batched fused step: one launch per batch step covers up to
 // kMarchShots shots, grouped by medium (and HABC width: one layout per
 // group).  Inside a group the shots' items are interleaved item-major
-// (block = item * n + shot), so the shots' copies of one (strip, segment) run
-// side by side and the medium's rows come from HBM once and from L2 for the
-// others.  The batch step comes from a device counter, so every launch of a
-// batch has the same parameters and a run of K steps can be captured once
-// into a CUDA graph: each block reads the counter first, and the last block to
-// finish advances it for the next launch.  Blocks of shots outside their step
-// range return at once; the receiver blocks record step ks-1 of each shot,
-// including the shot's last step one batch step later, exactly like the
-// split batch launches.
+// (item = strip-segment item * n + shot), so the shots' copies of one
+// (strip, segment) run side by side and the medium's rows come from HBM
+// once and from L2 for the others.  The batch step comes from a device
+// counter, so every launch of a batch has the same parameters and a run of
+// K steps can be captured once into a CUDA graph: each block reads the step
+// first, and the last block to leave advances it for the next launch.
+// Items of shots outside their step range are skipped; the receiver items
+// record step ks-1 of each shot, including the shot's last step one batch
+// step later, exactly like the split batch launches.
 constexpr int kMarchShots = 12;
 constexpr int kMarchGroups = 8;
 
@@ -577,15 +649,15 @@ struct MarchShot {
 struct MarchGroup {
     MarchArgs A;            // the group's layout, buoyancy and status word
     int first, n;           // shots first .. first+n-1
-    int item_off;           // the group's first block
+    int item_off;           // the group's first item
     int pad_;
 };
 
 struct BatchMarchLaunch {
-    int* step;              // batch step (1-based) of this launch
-    int* done;              // blocks of this launch finished so far
-    int n_shots, n_groups, total_items, pad_;
-    int rec_off[kMarchShots + 1];  // first receiver block of each shot (after the items)
+    int* step;              // step[0]: batch step (1-based) of this launch; step[1]: blocks left;
+                            // step[2]: next item
+    int n_shots, n_groups, total_items, n_rec_items;
+    int rec_off[kMarchShots + 1];  // first receiver item of each shot (after the strip-segment items)
     MarchGroup groups[kMarchGroups];
     MarchShot shot[kMarchShots];
     CUtensorMap tau[kMarchShots][2][3];  // tau boxes (TW x TH) of copy c
@@ -594,60 +666,58 @@ struct BatchMarchLaunch {
 static_assert(sizeof(BatchMarchLaunch) <= 32764, "kernel parameters above the 32764-byte limit");
 
 template <int M>
-__device__ __forceinline__ void batch_march_block(const BatchMarchLaunch& L, int step) {
-    const int bid = blockIdx.x;
-    if (bid < L.total_items) {
-        int g = 0;
-#pragma unroll 1
-        for (int h = 1; h < L.n_groups; ++h)
-            if (L.groups[h].item_off <= bid) g = h;
-        const MarchGroup& G = L.groups[g];
-        const int r = bid - G.item_off;
-        const int s = G.first + r % G.n, item = r / G.n;
-        const MarchShot& S = L.shot[s];
-        const int ks = step - S.start + 1;
-        if (ks < 1 || ks > S.nt) return;
-        const int a = (ks - 1) & 1;
-        int strip, seg;
-        march_item_of(G.A, item, &strip, &seg);
-        const MarchMapRefs mp{&L.tau[s][a][0], &L.tau[s][a][1], &L.tau[s][a][2], nullptr, nullptr, nullptr,
-                              nullptr,        nullptr,        nullptr,        nullptr, nullptr, nullptr, false};
-        const float src_w = ks <= S.n_wavelet ? __ldg(S.wavelet + ks - 1) : 0.f;
-        march_item<M>(S.P[a], G.A, mp, strip, seg, src_w);
-        return;
-    }
-    const int rb = bid - L.total_items;
-    if (rb >= L.rec_off[L.n_shots]) return;
-    int s = 0;
-#pragma unroll 1
-    while (L.rec_off[s + 1] <= rb) ++s;
-    const MarchShot& S = L.shot[s];
-    const int ks = step - S.start + 1;
-    if (ks >= 2 && ks <= S.nt + 1) record_block(S.P[(ks - 1) & 1], rb - L.rec_off[s], ks - 1);  // copy (ks-1)&1
-}
-
-template <int M>
 __global__ void __launch_bounds__(kMThreads, 2) batch_march_kernel(const __grid_constant__ BatchMarchLaunch L) {
+    __shared__ int s_item, s_err;
     const int step = *reinterpret_cast<volatile const int*>(L.step);
-    batch_march_block<M>(L, step);
-    __syncthreads();
-    if (threadIdx.x == 0) {  // every block has read the step once the last one gets here
-        __threadfence();
-        if (atomicAdd(L.done, 1) == (int)gridDim.x - 1) {
-            *L.done = 0;
-            *reinterpret_cast<volatile int*>(L.step) = step + 1;
-            __threadfence();
+    int* queue = L.step + 1;  // [0] next item, [1] blocks that left
+    int g = 0;
+    for (;;) {
+        const int item = march_next(queue, &s_item);
+        if (item >= L.total_items + L.n_rec_items) break;
+        if (item < L.total_items) {
+            int gi = 0;
+#pragma unroll 1
+            for (int h = 1; h < L.n_groups; ++h)
+                if (L.groups[h].item_off <= item) gi = h;
+            const MarchGroup& G = L.groups[gi];
+            const int r = item - G.item_off;
+            const int s = G.first + r % G.n;
+            const MarchShot& S = L.shot[s];
+            const int ks = step - S.start + 1;
+            if (ks >= 1 && ks <= S.nt) {
+                const int a = (ks - 1) & 1;
+                int strip, seg;
+                march_item_of(G.A, r / G.n, &strip, &seg);
+                const MarchMapRefs mp{&L.tau[s][a][0], &L.tau[s][a][1], &L.tau[s][a][2], nullptr, nullptr,
+                                      nullptr,         nullptr,         nullptr,         nullptr, nullptr,
+                                      nullptr,         nullptr,         false};
+                const float src_w = ks <= S.n_wavelet ? __ldg(S.wavelet + ks - 1) : 0.f;
+                if (!march_item<M>(S.P[a], G.A, mp, strip, seg, src_w, g, &s_err)) break;
+            }
+        } else {
+            const int rb = item - L.total_items;
+            int s = 0;
+#pragma unroll 1
+            while (L.rec_off[s + 1] <= rb) ++s;
+            const MarchShot& S = L.shot[s];
+            const int ks = step - S.start + 1;
+            if (ks >= 2 && ks <= S.nt + 1) record_block(S.P[(ks - 1) & 1], rb - L.rec_off[s], ks - 1);
         }
+        __syncthreads();
     }
+    // every block has read the step and taken its items once the last one leaves
+    if (march_leave(queue)) *reinterpret_cast<volatile int*>(L.step) = step + 1;
 }
 
-// Counters of n batched fused-step sets at a table rebuild: step of set i
-// (counters[2i]) = `step`, its finished-block count (counters[2i+1]) = 0.
+// Counters of n batched fused-step sets at a table rebuild: set i holds
+// counters[4i] = `step`, then its block count and its next item (zero).
 static __global__ void march_counters_kernel(int* counters, int n, int step) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) {
-        counters[2 * i] = step;
-        counters[2 * i + 1] = 0;
+        counters[4 * i] = step;
+        counters[4 * i + 1] = 0;
+        counters[4 * i + 2] = 0;
+        counters[4 * i + 3] = 0;
     }
 }
 

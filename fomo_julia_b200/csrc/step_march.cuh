@@ -295,6 +295,7 @@ __device__ __forceinline__ int march_v_hi(int vr0, int t, int n_it, int zb) {
 // items a block runs); it advances by the item's iterations.  The caller
 // has synchronised the block since its previous item.  Returns false (all
 // threads alike) if a TMA load did not land: the status word holds the error.
+// s_err: two shared words for the block's flag.
 template <int M>
 __device__ __forceinline__ bool march_item(const StepParams& P, const MarchArgs& A, const MarchMapRefs& mp,
                                            int strip, int seg, float src_w, int& g, int* s_err) {
@@ -331,7 +332,7 @@ __device__ __forceinline__ bool march_item(const StepParams& P, const MarchArgs&
     if (threadIdx.x == 0) {
         fence_proxy_async_smem();  // the previous item's generic accesses of the slots before the TMA refills them
         for (int t = 0; t < min(kMStages, n_it); ++t) march_issue<M>(A, mp, stage, full, x0, za, t, g0 + t);
-        *s_err = mbar_wait_parity(full + g0 % kMStages, (g0 / kMStages) & 1, A.status) ? 0 : 1;
+        s_err[0] = mbar_wait_parity(full + g0 % kMStages, (g0 / kMStages) & 1, A.status) ? 0 : 1;
     }
     // Pointwise operands of velocity block t, loaded one phase before they are used.
     float4 pvx = make_float4(0.f, 0.f, 0.f, 0.f), pvz = pvx, pb0 = pvx, pb1 = pvx, pb2 = pvx, pb3 = pvx;
@@ -349,7 +350,7 @@ __device__ __forceinline__ bool march_item(const StepParams& P, const MarchArgs&
     };
     load_v(0);
     __syncthreads();
-    if (*s_err) return false;
+    if (s_err[0]) return false;
 
     for (int t = 0; t < n_it; ++t) {
         const int gt = g0 + t;
@@ -458,10 +459,13 @@ __device__ __forceinline__ bool march_item(const StepParams& P, const MarchArgs&
         // velocity block t in the ring; every thread is done with iteration t-1.  Thread 0
         // waits for the next iteration's tau boxes here, so the other threads sleep in the
         // barrier instead of polling.
-        if (threadIdx.x == 0 && t + 1 < n_it)
-            *s_err = mbar_wait_parity(full + (gt + 1) % kMStages, ((gt + 1) / kMStages) & 1, A.status) ? 0 : 1;
+        // The flag alternates between two words, so a thread that reads it late still reads the
+        // word written before this barrier (thread 0 rewrites it only two barriers later).
+        if (threadIdx.x == 0)
+            s_err[(t + 1) & 1] =
+                t + 1 < n_it && !mbar_wait_parity(full + (gt + 1) % kMStages, ((gt + 1) / kMStages) & 1, A.status);
         __syncthreads();
-        if (*s_err) return false;
+        if (s_err[(t + 1) & 1]) return false;
         if (threadIdx.x == 0 && t >= 2 && t + 2 < n_it) {
             fence_proxy_async_smem();  // generic accesses of the slot before the TMA overwrites it
             march_issue<M>(A, mp, stage, full, x0, za, t + 2, gt + 2);
@@ -580,6 +584,20 @@ __device__ __forceinline__ bool march_item(const StepParams& P, const MarchArgs&
     return true;
 }
 
+// Thread 0 initialises the block's stage mbarriers once, before its first
+// item (their phases then run on across items: march_item's stage numbers);
+// the caller's next barrier publishes them.
+template <int M>
+__device__ __forceinline__ void march_init_barriers() {
+    using G = MGeo<M>;
+    extern __shared__ __align__(128) float smem[];
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem + kMStages * G::STAGE + 2 * G::RING + 3 * kMVW);
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < kMStages; ++s) mbar_init(full + s, 1);
+        fence_barrier_init();
+    }
+}
+
 // Work queue of a fused-step launch: a block takes items until none are
 // left; the last block to leave resets the queue for the next launch.
 __device__ __forceinline__ int march_next(int* queue, int* s_item) {
@@ -604,15 +622,16 @@ template <int M>
 __global__ void __launch_bounds__(kMThreads, 2)
     march_kernel(const __grid_constant__ StepParams P, const __grid_constant__ MarchArgs A,
                  const __grid_constant__ MarchMaps mp) {
-    __shared__ int s_item, s_err;
+    __shared__ int s_item, s_err[2];
     int g = 0;
+    march_init_barriers<M>();  // published by march_next's barrier
     for (;;) {
         const int item = march_next(A.queue, &s_item);
         if (item >= A.n_items + A.n_rec_items) break;
         if (item < A.n_items) {
             int strip, seg;
             march_item_of(A, item, &strip, &seg);
-            if (!march_item<M>(P, A, refs_of(mp), strip, seg, P.src_w, g, &s_err)) break;
+            if (!march_item<M>(P, A, refs_of(mp), strip, seg, P.src_w, g, s_err)) break;
         } else {
             record_block(P, item - A.n_items, P.rec_k);
         }
@@ -654,8 +673,8 @@ struct MarchGroup {
 };
 
 struct BatchMarchLaunch {
-    int* step;              // step[0]: batch step (1-based) of this launch; step[1]: blocks left;
-                            // step[2]: next item
+    int* step;              // step[0]: batch step (1-based) of this launch; step[1]: next item;
+                            // step[2]: blocks that left (both zero between launches)
     int n_shots, n_groups, total_items, n_rec_items;
     int rec_off[kMarchShots + 1];  // first receiver item of each shot (after the strip-segment items)
     MarchGroup groups[kMarchGroups];
@@ -667,10 +686,11 @@ static_assert(sizeof(BatchMarchLaunch) <= 32764, "kernel parameters above the 32
 
 template <int M>
 __global__ void __launch_bounds__(kMThreads, 2) batch_march_kernel(const __grid_constant__ BatchMarchLaunch L) {
-    __shared__ int s_item, s_err;
+    __shared__ int s_item, s_err[2];
     const int step = *reinterpret_cast<volatile const int*>(L.step);
     int* queue = L.step + 1;  // [0] next item, [1] blocks that left
     int g = 0;
+    march_init_barriers<M>();  // published by march_next's barrier
     for (;;) {
         const int item = march_next(queue, &s_item);
         if (item >= L.total_items + L.n_rec_items) break;
@@ -692,7 +712,7 @@ __global__ void __launch_bounds__(kMThreads, 2) batch_march_kernel(const __grid_
                                       nullptr,         nullptr,         nullptr,         nullptr, nullptr,
                                       nullptr,         nullptr,         false};
                 const float src_w = ks <= S.n_wavelet ? __ldg(S.wavelet + ks - 1) : 0.f;
-                if (!march_item<M>(S.P[a], G.A, mp, strip, seg, src_w, g, &s_err)) break;
+                if (!march_item<M>(S.P[a], G.A, mp, strip, seg, src_w, g, s_err)) break;
             }
         } else {
             const int rb = item - L.total_items;

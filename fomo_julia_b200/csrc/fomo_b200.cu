@@ -472,32 +472,34 @@ MarchPlan march_plan(int nx, int nz, int nbc, bool fs, int slots, int segs_req) 
     // the M rows its velocity reads above that.
     const int last_max = j0 - M;
     if (last_max < 0) return FOMO_NO("grid too shallow for the fused step");
+    if ((long)((nx + 31) / 32 * 32) * nz >= (1L << 31)) return FOMO_NO("grid too large for 32-bit cell offsets");
 #undef FOMO_NO
-    int ns = segs_req;
-    if (ns <= 0) {  // fewest whole waves x rows per segment (plus ~1.5 blocks of pipeline fill)
-        long best = -1;
-        for (int c = 1; c <= std::min(fomo::kMMaxSegs, std::max(1, nz / 32)); ++c) {
-            const long waves = ((long)S * c + slots - 1) / slots;
-            const long cost = waves * ((nz + c - 1) / c + 24);
-            if (best < 0 || cost < best) {
-                best = cost;
-                ns = c;
-            }
+    // One table of ns segments (at most kMMaxSegs, at least min_h rows each
+    // where the grid allows) whose last one starts at or above last_max.
+    auto segments = [&](int ns, int min_h, int* z) {
+        ns = std::max(1, std::min({ns, fomo::kMMaxSegs, std::max(1, nz / std::max(1, min_h))}));
+        for (;; --ns) {
+            const int h = (nz + ns - 1) / ns;
+            bool okz = true;
+            for (int q = 0; q < ns; ++q) z[q] = q * h;
+            z[ns] = nz;
+            if (ns > 1) z[ns - 1] = std::min(z[ns - 1], last_max);
+            for (int q = 0; q < ns; ++q) okz = okz && z[q + 1] > z[q];
+            if (okz || ns == 1) return ns;
         }
-    }
-    ns = std::max(1, std::min(ns, fomo::kMMaxSegs));
-    for (;; --ns) {
-        const int h = (nz + ns - 1) / ns;
-        bool okz = true;
-        for (int q = 0; q < ns; ++q) p.A.seg_z[q] = q * h;
-        p.A.seg_z[ns] = nz;
-        if (ns > 1) p.A.seg_z[ns - 1] = std::min(p.A.seg_z[ns - 1], last_max);
-        for (int q = 0; q < ns; ++q) okz = okz && p.A.seg_z[q + 1] > p.A.seg_z[q];
-        if (okz || ns == 1) break;
-    }
+    };
+    // Persistent blocks take items from a queue, so the segments only need to
+    // be short enough that every block gets several items (the last item of a
+    // block bounds the tail) and long enough to amortise the rows each item
+    // recomputes above it.  Edge strips apply the side HABC rules on almost
+    // every cell: their items are cut four times finer.
+    const int n_edge = std::min(S, 2);
+    const int ns = segs_req > 0 ? segs_req : (6 * slots + S - 1) / S;
+    p.A.n_segs = segments(ns, segs_req > 0 ? 1 : 48, p.A.seg_z);
+    p.A.n_segs_e = segments(segs_req > 0 ? segs_req : 4 * p.A.n_segs, segs_req > 0 ? 1 : 24, p.A.seg_ze);
     p.A.n_strips = S;
-    p.A.n_segs = ns;
-    p.A.n_items = S * ns;
+    p.A.n_edge = n_edge;
+    p.A.n_items = n_edge * p.A.n_segs_e + (S - n_edge) * p.A.n_segs;
     p.A.x_last = x_last;
     p.ok = true;
     return p;

@@ -60,8 +60,10 @@ struct MGeo {
     static constexpr int TH = kMR + 2 * M;          // tau box rows
     static constexpr int TAU = (TW * TH + 31) / 32 * 32;  // floats of one field's box (128-byte multiple)
     static constexpr int STAGE = 3 * TAU;
-    static constexpr int RING_ROWS = kMRing * kMR;  // 48
-    static constexpr int RING = RING_ROWS * kMVW;   // floats of one field's ring
+    static constexpr int RING_ROWS = kMRing * kMR;  // 48 rows of the ring proper
+    // The first 2M rows are mirrored after the ring, so a stress window (2M+1
+    // rows from any ring row) never wraps.
+    static constexpr int RING = (RING_ROWS + 2 * M) * kMVW;  // floats of one field's ring
 };
 
 // Launch-wide parameters of the fused step (besides StepParams).
@@ -73,7 +75,9 @@ struct MarchArgs {
     int n_rec_items;       // receiver items after the strip-segment items
     int n_strips, n_segs, n_items;
     int x_last;            // first output column of the last (right-aligned) strip
-    int seg_z[kMMaxSegs + 1];  // segment s: stress rows [seg_z[s], seg_z[s+1])
+    int n_edge, n_segs_e;  // edge strips (the first and the last: HABC side rules) and their segments
+    int seg_z[kMMaxSegs + 1];   // interior strips' segment s: stress rows [seg_z[s], seg_z[s+1])
+    int seg_ze[kMMaxSegs + 1];  // edge strips' segments (finer: their items cost more)
 };
 
 // Descriptors: tau boxes (TW x TH) of the step-start copy; L2-prefetch boxes
@@ -244,13 +248,22 @@ __device__ __forceinline__ MarchMapRefs refs_of(const MarchMaps& m) {
     return {&m.xx, &m.zz, &m.xz, &m.vx, &m.vz, &m.b0, &m.b1, &m.b2, &m.b3, &m.lam, &m.mu, &m.mxz, true};
 }
 
-// Item `item` of a shot's fused step: bottom segments first (they march the
-// band), and within a segment the two edge strips first (they apply the side
-// rules).
-__device__ __forceinline__ void march_item_of(const MarchArgs& A, int item, int* strip, int* seg) {
-    *seg = A.n_segs - 1 - item / A.n_strips;
-    const int k = item % A.n_strips;
-    *strip = k == 0 ? 0 : (k == 1 ? A.n_strips - 1 : k - 1);
+// Item `item` of a shot's fused step: the edge strips' items first (they
+// apply the side rules), then the interior strips'; bottom segments first in
+// each (they march the band).
+__device__ __forceinline__ void march_item_of(const MarchArgs& A, int item, int* strip, int* seg, bool* edge) {
+    const int ne = A.n_edge * A.n_segs_e;
+    if (item < ne) {
+        *edge = true;
+        *seg = A.n_segs_e - 1 - item / A.n_edge;
+        *strip = item % A.n_edge == 0 ? 0 : A.n_strips - 1;
+    } else {
+        item -= ne;
+        const int ni = A.n_strips - A.n_edge;
+        *edge = false;
+        *seg = A.n_segs - 1 - item / ni;
+        *strip = 1 + item % ni;
+    }
 }
 
 // Thread 0: TMA loads of the tau boxes of iteration t (the block's stage
@@ -298,19 +311,20 @@ __device__ __forceinline__ int march_v_hi(int vr0, int t, int n_it, int zb) {
 // s_err: two shared words for the block's flag.
 template <int M>
 __device__ __forceinline__ bool march_item(const StepParams& P, const MarchArgs& A, const MarchMapRefs& mp,
-                                           int strip, int seg, float src_w, int& g, int* s_err) {
+                                           int strip, int seg, bool edge, float src_w, int& g, int* s_err) {
     using G = MGeo<M>;
     extern __shared__ __align__(128) float smem[];
     const bool last_strip = strip == A.n_strips - 1;
     const int x0 = last_strip ? A.x_last : strip * G::W;
     const int x_end = last_strip ? min(x0 + G::W, (P.nx + 3) / 4 * 4) : min(x0 + G::W, A.x_last);
     const int xa = x0 - G::HV;
-    const int za = A.seg_z[seg], zb = A.seg_z[seg + 1];
+    const int* segz = edge ? A.seg_ze : A.seg_z;
+    const int za = segz[seg], zb = segz[seg + 1];
     const int n_it = (zb - za + kMR - 1) / kMR + 1;  // velocity blocks 0..n_it-1; stress blocks 0..n_it-2
     const int nx = P.nx, nz = P.nz, b = P.nbc;
     const int j0 = nz - b - 1;                        // first bottom-band row
-    const int edge = max(b + 2, M);
-    const bool side = xa < edge || xa + kMVW > nx - edge;  // block-uniform: side HABC or rim columns
+    const int ecols = max(b + 2, M);
+    const bool side = xa < ecols || xa + kMVW > nx - ecols;  // block-uniform: side HABC or rim columns
     const int g0 = g;
     g += n_it;
 
@@ -339,7 +353,7 @@ __device__ __forceinline__ bool march_item(const StepParams& P, const MarchArgs&
     auto load_v = [&](int t) {
         const int j = za - M + t * kMR + ty;
         if (v_in && j >= 0 && j < nz && j < march_v_hi<M>(za - M + t * kMR, t, n_it, zb)) {
-            const size_t c = cell(P, xv, j);
+            const int c = xv + j * P.pitch;  // 32-bit offsets (march_plan: pitch * nz < 2^31)
             pvx = ldg4(P.in[VX] + c);
             pvz = ldg4(P.in[VZ] + c);
             pb0 = ldg4(A.b[0] + c);
@@ -363,7 +377,7 @@ __device__ __forceinline__ bool march_item(const StepParams& P, const MarchArgs&
         const bool s_row = t >= 1 && js < zb && js < nz;
         float4 mlam = make_float4(0.f, 0.f, 0.f, 0.f), mmu = mlam, mmxz = mlam;
         if (s_row && s_in) {
-            const size_t c = cell(P, xs, js);
+            const int c = xs + js * P.pitch;
             mlam = ldg4(P.lam + c);
             mmu = ldg4(P.mu_txx + c);
             mmxz = ldg4(P.mu_txz + c);
@@ -449,11 +463,15 @@ __device__ __forceinline__ bool march_item(const StepParams& P, const MarchArgs&
                     oz = *reinterpret_cast<const float4*>(rvz);
                 }
             }
+            if (slot == 0 && ty < 2 * M) {  // the mirror of the ring's first rows
+                *reinterpret_cast<float4*>(rvx + G::RING_ROWS * kMVW) = ox;
+                *reinterpret_cast<float4*>(rvz + G::RING_ROWS * kMVW) = oz;
+            }
             // the segment's own rows (the rows above are the previous segment's); band rows were
             // stored by the march
             if (row_ok && v_own && j >= za && j < zb && !(j >= j0 && j <= nz - 2)) {
-                stg4(P.out[VX] + cell(P, xv, j), ox);
-                stg4(P.out[VZ] + cell(P, xv, j), oz);
+                stg4(P.out[VX] + (xv + j * P.pitch), ox);
+                stg4(P.out[VZ] + (xv + j * P.pitch), oz);
             }
         }
         // velocity block t in the ring; every thread is done with iteration t-1.  Thread 0
@@ -481,14 +499,11 @@ __device__ __forceinline__ bool march_item(const StepParams& P, const MarchArgs&
                 const int bo = (ty + 2 * M) * G::TW + 2 * G::HV + 4 * tx;
                 const float4 txx = lds4(told + bo), tzz = lds4(told + G::TAU + bo);
                 const float4 txz = lds4(told + 2 * G::TAU + bo);
-                // ring row of grid row j - M + q: r + q, wrapped once at the ring's end
+                // ring row of grid row j - M + q: r + q
                 const int r = ((t - 1) % kMRing) * kMR + ty;
                 const float* rvx = ring + 4 * tx;
                 const float* rvz = ring + G::RING + 4 * tx;
-                auto rrow = [&](int q) {
-                    const int x = r + q;
-                    return (x >= G::RING_ROWS ? x - G::RING_ROWS : x) * kMVW;
-                };
+                auto rrow = [&](int q) { return (r + q) * kMVW; };  // rows past the ring are its mirror
                 const float4 dxx = xderiv1<M, 1>(P, rvx + rrow(M));  // vx[i+l] - vx[i-l+1]
                 const float4 dzx = xderiv1<M, 0>(P, rvz + rrow(M));  // vz[i+l-1] - vz[i-l]
                 float4 wz[2 * M];
@@ -575,9 +590,9 @@ __device__ __forceinline__ bool march_item(const StepParams& P, const MarchArgs&
                     ozz = make_float4(0.f, 0.f, 0.f, 0.f);
                     oxz = ozz;
                 }
-                stg4(P.out[TXX] + cell(P, xs, j), oxx);
-                stg4(P.out[TZZ] + cell(P, xs, j), ozz);
-                stg4(P.out[TXZ] + cell(P, xs, j), oxz);
+                stg4(P.out[TXX] + (xs + j * P.pitch), oxx);
+                stg4(P.out[TZZ] + (xs + j * P.pitch), ozz);
+                stg4(P.out[TXZ] + (xs + j * P.pitch), oxz);
             }
         }
     }
@@ -630,8 +645,9 @@ __global__ void __launch_bounds__(kMThreads, 2)
         if (item >= A.n_items + A.n_rec_items) break;
         if (item < A.n_items) {
             int strip, seg;
-            march_item_of(A, item, &strip, &seg);
-            if (!march_item<M>(P, A, refs_of(mp), strip, seg, P.src_w, g, s_err)) break;
+            bool edge;
+            march_item_of(A, item, &strip, &seg, &edge);
+            if (!march_item<M>(P, A, refs_of(mp), strip, seg, edge, P.src_w, g, s_err)) break;
         } else {
             record_block(P, item - A.n_items, P.rec_k);
         }
@@ -707,12 +723,13 @@ __global__ void __launch_bounds__(kMThreads, 2) batch_march_kernel(const __grid_
             if (ks >= 1 && ks <= S.nt) {
                 const int a = (ks - 1) & 1;
                 int strip, seg;
-                march_item_of(G.A, r / G.n, &strip, &seg);
+                bool edge;
+                march_item_of(G.A, r / G.n, &strip, &seg, &edge);
                 const MarchMapRefs mp{&L.tau[s][a][0], &L.tau[s][a][1], &L.tau[s][a][2], nullptr, nullptr,
                                       nullptr,         nullptr,         nullptr,         nullptr, nullptr,
                                       nullptr,         nullptr,         false};
                 const float src_w = ks <= S.n_wavelet ? __ldg(S.wavelet + ks - 1) : 0.f;
-                if (!march_item<M>(S.P[a], G.A, mp, strip, seg, src_w, g, s_err)) break;
+                if (!march_item<M>(S.P[a], G.A, mp, strip, seg, edge, src_w, g, s_err)) break;
             }
         } else {
             const int rb = item - L.total_items;

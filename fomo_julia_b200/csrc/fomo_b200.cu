@@ -13,7 +13,9 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <memory>
+#include <tuple>
 #include <utility>
 #include <mutex>
 #include <string>
@@ -610,15 +612,63 @@ MarchPlan shot_march_plan(const Shot& s, const Medium& m) {
 }
 
 template <int M>
-int run_steps_M(Shot& s, Medium& m, Wavefield& w, int n_steps, Profile* prof) {
-    {
-        const MarchPlan plan = shot_march_plan<M>(s, m);
-        if (plan.ok) {
-            if constexpr (M <= 4) return run_steps_march<M>(s, m, w, n_steps, prof, plan);
-        } else if (g_step_mode.load() == FOMO_STEP_FUSED) {
-            return fail(FOMO_EINVAL, "the fused step does not support this shot: %s", plan.why);
-        }
+int run_steps_split(Shot& s, Medium& m, Wavefield& w, int n_steps, Profile* prof);
+
+// FOMO_STEP_AUTO's choice per grid and HABC width, made once per process by
+// timing both kernels on live steps of the first shot (they give the same
+// bits, so the shot itself is unaffected): 0 = split launches, 1 = fused.
+struct StepKey {
+    int nx, nz, M, nbc, fs, iso;
+    bool operator<(const StepKey& o) const {
+        return std::tie(nx, nz, M, nbc, fs, iso) < std::tie(o.nx, o.nz, o.M, o.nbc, o.fs, o.iso);
     }
+};
+std::mutex g_step_choice_mu;
+std::map<StepKey, int> g_step_choice;
+constexpr int kStepTuneWindow = 24;  // steps timed per candidate
+
+template <int M>
+int run_steps_M(Shot& s, Medium& m, Wavefield& w, int n_steps, Profile* prof) {
+    const int mode = g_step_mode.load();
+    const MarchPlan plan = shot_march_plan<M>(s, m);
+    if (!plan.ok) {
+        if (mode == FOMO_STEP_FUSED) return fail(FOMO_EINVAL, "the fused step does not support this shot: %s", plan.why);
+        return run_steps_split<M>(s, m, w, n_steps, prof);
+    }
+    if constexpr (M <= 4) {
+        const StepKey key{m.nx, m.nz, M, s.nbc, m.fs, s.dtx == s.dtz};
+        int choice = mode == FOMO_STEP_FUSED ? 1 : -1;
+        if (choice < 0) {
+            std::lock_guard<std::mutex> lk(g_step_choice_mu);
+            auto it = g_step_choice.find(key);
+            if (it != g_step_choice.end()) choice = it->second;
+        }
+        if (choice < 0) {
+            const int W = kStepTuneWindow;
+            if (prof || std::min(n_steps, s.nt - s.k_done) < 3 * W) {
+                choice = 0;  // too few steps to time both: the split launches, nothing recorded
+            } else {
+                double t0 = s.device_ms;
+                if (int rc = run_steps_march<M>(s, m, w, W, nullptr, plan)) return rc;
+                const double t_fused = s.device_ms - t0;
+                t0 = s.device_ms;
+                if (int rc = run_steps_split<M>(s, m, w, W, nullptr)) return rc;
+                const double t_split = s.device_ms - t0;
+                choice = t_fused < t_split ? 1 : 0;
+                n_steps -= 2 * W;
+                std::lock_guard<std::mutex> lk(g_step_choice_mu);
+                g_step_choice[key] = choice;
+            }
+        }
+        if (choice == 1) return run_steps_march<M>(s, m, w, n_steps, prof, plan);
+    }
+    return run_steps_split<M>(s, m, w, n_steps, prof);
+}
+
+// The split launches: velocity tiles, velocity band pass, stress tiles,
+// stress band pass per step.
+template <int M>
+int run_steps_split(Shot& s, Medium& m, Wavefield& w, int n_steps, Profile* prof) {
     auto& C = ctx();
     const bool iso = s.dtx == s.dtz;
     const Launch L = launch_shape<M>(m.nx, m.nz, s.nbc, iso, m.fs != 0);

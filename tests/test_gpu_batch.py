@@ -63,9 +63,9 @@ def source_xs(c: Case, n):
 MEDIUM_A = dict(nx_in=231, nz_in=90, seed=13, nbc=10, fd_order=8, nt=100, n_rec=41)
 
 
-@pytest.fixture(params=["auto", "split"])
+@pytest.fixture(params=["fused", "split"])
 def step_mode(request):
-    """Fused-step launches ("auto" on this medium) and the split launches."""
+    """Fused-step batch launches and the split launches ("auto" runs the split ones)."""
     F.set_step_kernel(request.param)
     yield request.param
     F.set_step_kernel("auto")
@@ -81,7 +81,7 @@ def test_batch_equals_single_shots_and_oracle(b200, oracle_lib, step_mode):
     assert res[0].stats["steps"] == len(xs) * c.nt
     # one fused launch per batch step, or four split launches (tiles and band passes of both half steps)
     per_step = res[0].stats["kernel_launches"] / c.nt
-    assert (per_step < 2.5) == (step_mode == "auto"), per_step
+    assert (per_step < 2.5) == (step_mode == "fused"), per_step
     for k, r in enumerate(res):
         src = F.create_source(S.med, cfg.shots[k], cfg.wavelet)
         assert (r.src_i, r.src_j) == (src.i, src.j)

@@ -130,13 +130,22 @@ def step_kernel():
 
 @pytest.mark.parametrize("c", CASES, ids=lambda c: c.name)
 def test_shot_matches_oracle(c, b200, oracle_lib):
-    # "auto": the fused step where it applies, the split launches elsewhere
+    # "auto": the split launches, or the fused step where it applies and was timed faster
+    # on the grid (the first shot of a grid times both on its first steps)
     r, f_gpu = gpu_run(c, b200)
     g_orc, f_orc = oracle_run(c, oracle_lib)
     assert_same(r.gather, g_orc, f_gpu, f_orc)
     assert r.stats["steps"] == c.nt
-    launches_per_step = r.stats["kernel_launches"] / c.nt
-    assert (launches_per_step < 1.5) == fused_supported(c), launches_per_step
+
+
+@pytest.mark.parametrize("c", [c for c in CASES if fused_supported(c)], ids=lambda c: c.name)
+def test_fused_step_matches_oracle(c, b200, oracle_lib, step_kernel):
+    # one launch per step: velocity, stress and every boundary rule in the fused kernel
+    step_kernel("fused")
+    r, f_gpu = gpu_run(c, b200)
+    g_orc, f_orc = oracle_run(c, oracle_lib)
+    assert_same(r.gather, g_orc, f_gpu, f_orc)
+    assert r.stats["kernel_launches"] <= c.nt + 1
 
 
 @pytest.mark.parametrize("c", [c for c in CASES if fused_supported(c)], ids=lambda c: c.name)

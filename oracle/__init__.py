@@ -83,6 +83,8 @@ def lib():
         L.orc_run_shot_f32.argtypes = [ctypes.POINTER(OrcShot), P, P, ctypes.c_int]
         L.orc_run_shot_f64.argtypes = [ctypes.POINTER(OrcShot), P, P, ctypes.c_int]
         L.orc_max_threads.restype = ctypes.c_int
+        L.orc_create_geometry.argtypes = ([ctypes.c_int] * 3 + [P, P, ctypes.c_int, ctypes.c_float, ctypes.c_float,
+                                           ctypes.c_float, ctypes.c_int, ctypes.c_int, ctypes.c_int] + [P] * 6)
         _lib = L
     return _lib
 
@@ -188,6 +190,24 @@ def coord_to_index(x: float, dx: float, pad: int) -> int:
     """round(Int, x/dx) + pad + 1, Float32 division, ties to even
     (src/utils/init.jl:220-221, src/simulation/shot_manager.jl:189-191)."""
     return int(lib().orc_coord_to_index(float(np.float32(x)), float(np.float32(dx)), int(pad)))
+
+
+def create_geometry(src_i, src_j, rec_i, rec_j, pad, dx, dz, dt, nt, nx, nz) -> dict:
+    """create_geometry (src/io/geometry_io.jl:85-130) for one shot's 1-based
+    padded-grid indices: discretised coordinates, indices relative to the
+    physical domain, t_max and the physical grid size."""
+    ri = np.ascontiguousarray(rec_i, dtype=np.int32)
+    rj = np.ascontiguousarray(rec_j, dtype=np.int32)
+    n = ri.size
+    gf = np.zeros(3, np.float32)
+    gi = np.zeros(4, np.int32)
+    rx, rz = np.zeros(n, np.float32), np.zeros(n, np.float32)
+    rip, rjp = np.zeros(n, np.int32), np.zeros(n, np.int32)
+    lib().orc_create_geometry(int(src_i), int(src_j), n, _p(ri), _p(rj), int(pad), float(np.float32(dx)),
+                              float(np.float32(dz)), float(np.float32(dt)), int(nt), int(nx), int(nz),
+                              _p(gf), _p(gi), _p(rx), _p(rz), _p(rip), _p(rjp))
+    return dict(src_x=gf[0], src_z=gf[1], t_max=gf[2], src_i=int(gi[0]), src_j=int(gi[1]), nx=int(gi[2]),
+                nz=int(gi[3]), rec_x=rx, rec_z=rz, rec_i=rip, rec_j=rjp)
 
 
 # --------------------------------------------------------------------------

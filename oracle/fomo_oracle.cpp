@@ -697,6 +697,36 @@ int orc_run_shot_f64(const OrcShot* p, double* gather, double* final_fields, int
     return run_shot<double>(p, gather, final_fields, n_steps);
 }
 
+// create_geometry (src/io/geometry_io.jl:85-130) for one shot: coordinates
+// are the discretised positions (index - pad - 1) * dx, the Int converted to
+// Float32 and multiplied once in Float32 (:90-95); indices relative to the
+// physical domain are index - pad (:98-101); t_max = dt * nt, the Int
+// converted to Float32 (:107); the physical grid is nx - 2 pad by nz - 2 pad
+// (:109).  geo_f = [src_x, src_z, t_max], geo_i = [src_i, src_j, nx, nz].
+void orc_create_geometry(int src_i, int src_j, int n_rec, const int* rec_i, const int* rec_j, int pad, float dx,
+                         float dz, float dt, int nt, int nx, int nz, float* geo_f, int* geo_i, float* rec_x,
+                         float* rec_z, int* rec_i_phys, int* rec_j_phys) {
+    volatile float t;  // each product rounded to Float32 on its own
+    t = (float)(src_i - pad - 1) * dx;
+    geo_f[0] = t;
+    t = (float)(src_j - pad - 1) * dz;
+    geo_f[1] = t;
+    t = dt * (float)nt;
+    geo_f[2] = t;
+    geo_i[0] = src_i - pad;
+    geo_i[1] = src_j - pad;
+    geo_i[2] = nx - 2 * pad;
+    geo_i[3] = nz - 2 * pad;
+    for (int r = 0; r < n_rec; ++r) {
+        t = (float)(rec_i[r] - pad - 1) * dx;
+        rec_x[r] = t;
+        t = (float)(rec_j[r] - pad - 1) * dz;
+        rec_z[r] = t;
+        rec_i_phys[r] = rec_i[r] - pad;
+        rec_j_phys[r] = rec_j[r] - pad;
+    }
+}
+
 int orc_max_threads(void) {
 #ifdef _OPENMP
     return omp_get_max_threads();

@@ -9,6 +9,7 @@ import json
 import numpy as np
 import pytest
 
+import fomo_julia_b200 as F
 from fomo_julia_b200 import geometry as G
 from fomo_julia_b200.elastic2d import ShotResult
 
@@ -131,3 +132,25 @@ def test_multi_shot_json_and_txt(tmp_path):
         G.save_geometry(str(tmp_path / "s.jld2"), mg)
     with pytest.raises(ValueError):
         G.save_geometry(str(tmp_path / "s.xyz"), mg)
+
+
+@pytest.mark.parametrize("seed", [0, 1, 2])
+def test_create_geometry_matches_oracle(seed, oracle_lib):
+    # geometry_io.jl:85-130 restated in the oracle: coordinates, indices, t_max, grid size
+    rng = np.random.default_rng(seed)
+    pad = int(rng.integers(5, 60))
+    dx, dz = f32(rng.choice([10.0, 12.5, 7.3])), f32(rng.choice([10.0, 12.5, 3.1]))
+    dt, nt = f32(rng.uniform(1e-4, 2e-3)), int(rng.integers(100, 20000))
+    nx, nz = int(rng.integers(2 * pad + 10, 5000)), int(rng.integers(2 * pad + 10, 4000))
+    n_rec = int(rng.integers(1, 500))
+    ri = rng.integers(1, nx + 1, n_rec)
+    rj = rng.integers(1, nz + 1, n_rec)
+    si, sj = int(rng.integers(1, nx + 1)), int(rng.integers(1, nz + 1))
+    med = F.Medium(nx, nz, float(dx), float(dz), 0.0, 0.0, 4, pad, True, *[None] * 5)
+    par = F.sim_params(dt, nt, float(dx), float(dz), 8)
+    g = G.create_geometry(ShotResult(np.zeros((1, n_rec), f32), 3, si, sj, ri, rj), med, par)
+    o = oracle_lib.create_geometry(si, sj, ri, rj, pad, dx, dz, dt, nt, nx, nz)
+    assert (g.src_x, g.src_z, g.t_max) == (o["src_x"], o["src_z"], o["t_max"])
+    assert (g.src_i, g.src_j, g.nx, g.nz) == (o["src_i"], o["src_j"], o["nx"], o["nz"])
+    assert np.array_equal(g.rec_x, o["rec_x"]) and np.array_equal(g.rec_z, o["rec_z"])
+    assert np.array_equal(g.rec_i_idx, o["rec_i"]) and np.array_equal(g.rec_j_idx, o["rec_j"])

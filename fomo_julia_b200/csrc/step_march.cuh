@@ -46,7 +46,8 @@ namespace fomo {
 
 constexpr int kMR = 16;            // rows per block
 constexpr int kMVW = 64;           // velocity columns of a strip, halo included
-constexpr int kMThreads = 256;     // 16 column groups x 16 rows, one row per thread
+constexpr int kMRowsPerThread = 2;  // rows of a 16-row block each thread updates (4 columns each)
+constexpr int kMThreads = 16 * kMR / kMRowsPerThread;  // 16 column groups x 16 rows
 constexpr int kMStages = 4;        // tau box stages
 constexpr int kMRing = 3;          // velocity blocks kept
 constexpr int kMMaxSegs = 64;
@@ -173,7 +174,6 @@ struct SmemRows {
     }
 };
 
-constexpr int kMarchWarps = 6;  // warps that run the band recurrence (fields x 28-column strips)
 
 // The bottom-band recurrence (rows nz-nbc-1 .. nz-2) of one field over the
 // band rows [ja, jb) of one block: `pre` holds the block's values after the
@@ -182,11 +182,13 @@ constexpr int kMarchWarps = 6;  // warps that run the band recurrence (fields x 
 // xs - 2 + l; lanes 2..29 write back, and store their own columns
 // [own_lo, own_hi).  Columns [c_lo, c_hi) hold values.  `prev` (column 0 =
 // pre_xs), when given, holds the finals of row ja - 1; otherwise that row is
-// read from `pre`.  The lane rules are band_march's.
+// read from `pre`.  The n_warps warps of one field (its strips) call it
+// together: they meet at a named barrier between reading and writing back.
+// The lane rules are band_march's.
 __device__ __forceinline__ void march_band_rows(const StepParams& P, const float* tab, const float* oin, float* oout,
                                                 float* pre, int pre_pitch, int pre_xs, int pre_z0, int pre_r0,
                                                 int pre_rows, int c_lo, int c_hi, int own_lo, int own_hi, int xs,
-                                                int ja, int jb, const float* prev) {
+                                                int ja, int jb, const float* prev, int n_warps) {
     constexpr unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const int b = P.nbc, nx = P.nx, nz = P.nz, r0 = nx - b - 1;
@@ -213,7 +215,7 @@ __device__ __forceinline__ void march_band_rows(const StepParams& P, const float
     float pvs[kMR];
 #pragma unroll
     for (int r = 0; r < kMR; ++r) pvs[r] = (have && ja + r < jb) ? *at(ja + r) : 0.f;
-    asm volatile("bar.sync 1, %0;" ::"n"(kMarchWarps * 32) : "memory");
+    asm volatile("bar.sync 1, %0;" ::"r"(n_warps * 32) : "memory");  // the n_warps warps of this round
 #pragma unroll
     for (int r = 0; r < kMR; ++r) {
         const int j = ja + r;
@@ -302,17 +304,38 @@ __device__ __forceinline__ int march_v_hi(int vr0, int t, int n_it, int zb) {
     return min(vr0 + (t < n_it - 1 ? kMR : 2 * M), zb + M);
 }
 
+// z-derivatives of RT consecutive rows from a (2M + RT - 1)-row window:
+// d[rr] = sum_l a_l (w[rr+M+l-1] - w[rr+M-l]), in the reference's order.
+template <int M, int RT>
+__device__ __forceinline__ void zderivR(const StepParams& P, const float4 (&w)[2 * M + RT - 1], float4 (&d)[RT]) {
+#pragma unroll
+    for (int rr = 0; rr < RT; ++rr) {
+        float4 a = make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+        for (int l = 1; l <= M; ++l) {
+            const float al = P.a[l - 1];
+            a.x = fadd(fmul(al, fsub(w[rr + M + l - 1].x, w[rr + M - l].x)), a.x);
+            a.y = fadd(fmul(al, fsub(w[rr + M + l - 1].y, w[rr + M - l].y)), a.y);
+            a.z = fadd(fmul(al, fsub(w[rr + M + l - 1].z, w[rr + M - l].z)), a.z);
+            a.w = fadd(fmul(al, fsub(w[rr + M + l - 1].w, w[rr + M - l].w)), a.w);
+        }
+        d[rr] = a;
+    }
+}
+
 // One (strip, segment) of a shot's time step; src_w is the wavelet sample
 // added to txx and tzz at the source cell this step.  g is the block's
 // running stage number (stage slots and mbarrier phases continue across the
 // items a block runs); it advances by the item's iterations.  The caller
 // has synchronised the block since its previous item.  Returns false (all
 // threads alike) if a TMA load did not land: the status word holds the error.
-// s_err: two shared words for the block's flag.
+// s_err: two shared words for the block's flag.  Each thread updates 4
+// columns x kMRowsPerThread rows of every 16-row block.
 template <int M>
 __device__ __forceinline__ bool march_item(const StepParams& P, const MarchArgs& A, const MarchMapRefs& mp,
                                            int strip, int seg, bool edge, float src_w, int& g, int* s_err) {
     using G = MGeo<M>;
+    constexpr int RT = kMRowsPerThread;
     extern __shared__ __align__(128) float smem[];
     const bool last_strip = strip == A.n_strips - 1;
     const int x0 = last_strip ? A.x_last : strip * G::W;
@@ -321,7 +344,7 @@ __device__ __forceinline__ bool march_item(const StepParams& P, const MarchArgs&
     const int* segz = edge ? A.seg_ze : A.seg_z;
     const int za = segz[seg], zb = segz[seg + 1];
     const int n_it = (zb - za + kMR - 1) / kMR + 1;  // velocity blocks 0..n_it-1; stress blocks 0..n_it-2
-    const int nx = P.nx, nz = P.nz, b = P.nbc;
+    const int nx = P.nx, nz = P.nz, b = P.nbc, pitch = P.pitch;
     const int j0 = nz - b - 1;                        // first bottom-band row
     const int ecols = max(b + 2, M);
     const bool side = xa < ecols || xa + kMVW > nx - ecols;  // block-uniform: side HABC or rim columns
@@ -329,11 +352,12 @@ __device__ __forceinline__ bool march_item(const StepParams& P, const MarchArgs&
     g += n_it;
 
     float* stage = smem;
-    float* ring = smem + kMStages * G::STAGE;          // [2 fields][48 rows][64]
+    float* ring = smem + kMStages * G::STAGE;          // [2 fields][48 rows + mirror][64]
     float* s_last = ring + 2 * G::RING;                // [3][64] stress finals of a block's last row
     uint64_t* full = reinterpret_cast<uint64_t*>(s_last + 3 * kMVW);
 
-    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+    const int tx = threadIdx.x & 15, rp = threadIdx.x >> 4;
+    const int ty = rp * RT;              // the thread's first row within a 16-row block
     const int xv = xa + 4 * tx;          // first column of the thread's velocity cells
     const int xs = x0 + 4 * tx;          // first column of the thread's stress cells (tx < W/4)
     const bool s_col = tx < G::W / 4;
@@ -349,17 +373,23 @@ __device__ __forceinline__ bool march_item(const StepParams& P, const MarchArgs&
         s_err[0] = mbar_wait_parity(full + g0 % kMStages, (g0 / kMStages) & 1, A.status) ? 0 : 1;
     }
     // Pointwise operands of velocity block t, loaded one phase before they are used.
-    float4 pvx = make_float4(0.f, 0.f, 0.f, 0.f), pvz = pvx, pb0 = pvx, pb1 = pvx, pb2 = pvx, pb3 = pvx;
+    float4 pvx[RT], pvz[RT], pb0[RT], pb1[RT], pb2[RT], pb3[RT];
     auto load_v = [&](int t) {
-        const int j = za - M + t * kMR + ty;
-        if (v_in && j >= 0 && j < nz && j < march_v_hi<M>(za - M + t * kMR, t, n_it, zb)) {
-            const int c = xv + j * P.pitch;  // 32-bit offsets (march_plan: pitch * nz < 2^31)
-            pvx = ldg4(P.in[VX] + c);
-            pvz = ldg4(P.in[VZ] + c);
-            pb0 = ldg4(A.b[0] + c);
-            pb2 = ldg4(A.b[2] + c);
-            pb1 = A.iso ? pb0 : ldg4(A.b[1] + c);
-            pb3 = A.iso ? pb2 : ldg4(A.b[3] + c);
+        const int vr = za - M + t * kMR;
+        const int hi = march_v_hi<M>(vr, t, n_it, zb);
+#pragma unroll
+        for (int rr = 0; rr < RT; ++rr) {
+            const int j = vr + ty + rr;
+            pvx[rr] = pvz[rr] = pb0[rr] = pb1[rr] = pb2[rr] = pb3[rr] = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (v_in && j >= 0 && j < nz && j < hi) {
+                const int c = xv + j * pitch;  // 32-bit offsets (march_plan: pitch * nz < 2^31)
+                pvx[rr] = ldg4(P.in[VX] + c);
+                pvz[rr] = ldg4(P.in[VZ] + c);
+                pb0[rr] = ldg4(A.b[0] + c);
+                pb2[rr] = ldg4(A.b[2] + c);
+                pb1[rr] = A.iso ? pb0[rr] : ldg4(A.b[1] + c);
+                pb3[rr] = A.iso ? pb2[rr] : ldg4(A.b[3] + c);
+            }
         }
     };
     load_v(0);
@@ -373,14 +403,19 @@ __device__ __forceinline__ bool march_item(const StepParams& P, const MarchArgs&
         const int slot = t % kMRing;
         // medium of stress block t-1, loaded now and used after the velocity
         const int sr0 = za + (t - 1) * kMR;
-        const int js = sr0 + ty;
-        const bool s_row = t >= 1 && js < zb && js < nz;
-        float4 mlam = make_float4(0.f, 0.f, 0.f, 0.f), mmu = mlam, mmxz = mlam;
-        if (s_row && s_in) {
-            const int c = xs + js * P.pitch;
-            mlam = ldg4(P.lam + c);
-            mmu = ldg4(P.mu_txx + c);
-            mmxz = ldg4(P.mu_txz + c);
+        float4 mlam[RT], mmu[RT], mmxz[RT];
+        bool s_row[RT];
+#pragma unroll
+        for (int rr = 0; rr < RT; ++rr) {
+            const int js = sr0 + ty + rr;
+            s_row[rr] = t >= 1 && js < zb && js < nz;
+            mlam[rr] = mmu[rr] = mmxz[rr] = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (s_row[rr] && s_in) {
+                const int c = xs + js * pitch;
+                mlam[rr] = ldg4(P.lam + c);
+                mmu[rr] = ldg4(P.mu_txx + c);
+                mmxz[rr] = ldg4(P.mu_txz + c);
+            }
         }
         // ------------------------------------------------ the source, into this stage's copy
         {
@@ -395,90 +430,124 @@ __device__ __forceinline__ bool march_item(const StepParams& P, const MarchArgs&
         }
         // ------------------------------------------------ velocity block t
         {
-            const int j = vr0 + ty;
             const int v_hi = march_v_hi<M>(vr0, t, n_it, zb);
-            float4 ox = make_float4(0.f, 0.f, 0.f, 0.f), oz = ox;
-            const bool row_ok = j < v_hi && j >= 0 && j < nz;
-            if (row_ok && v_in) {
-                const float* rxx = tau + (ty + M) * G::TW + 4 * tx;  // windows from column xv - 4
-                const float* rxz = tau + 2 * G::TAU + (ty + M) * G::TW + 4 * tx;
-                const float4 d1 = xderiv1<M, 0>(P, rxx);   // dtxx/dx: txx[i+l-1] - txx[i-l]
-                const float4 d3 = xderiv1<M, 1>(P, rxz);   // dtxz/dx: txz[i+l] - txz[i-l+1]
-                float4 wz[2 * M];
+            float4 ox[RT], oz[RT];
+            bool row_ok[RT];
+            bool any = false;
 #pragma unroll
-                for (int q = 0; q < 2 * M; ++q) wz[q] = lds4(tau + 2 * G::TAU + (ty + q) * G::TW + 4 * tx + G::HV);
-                const float4 d2 = zderiv1<M>(P, wz);        // dtxz/dz: txz[j+l-1] - txz[j-l]
+            for (int rr = 0; rr < RT; ++rr) {
+                const int j = vr0 + ty + rr;
+                row_ok[rr] = j < v_hi && j >= 0 && j < nz;
+                any = any || row_ok[rr];
+                ox[rr] = oz[rr] = make_float4(0.f, 0.f, 0.f, 0.f);
+            }
+            if (any && v_in) {
+                float4 d1[RT], d3[RT];
 #pragma unroll
-                for (int q = 0; q < 2 * M; ++q) wz[q] = lds4(tau + G::TAU + (ty + 1 + q) * G::TW + 4 * tx + G::HV);
-                const float4 d4 = zderiv1<M>(P, wz);        // dtzz/dz: tzz[j+l] - tzz[j-l+1]
-                ox = add4(pvx, add4(mul4(pb0, d1), mul4(pb1, d2)));
-                oz = add4(pvz, add4(mul4(pb2, d3), mul4(pb3, d4)));
-                if (side || j < M || j > nz - 1 - M) {
+                for (int rr = 0; rr < RT; ++rr) {
+                    const float* rxx = tau + (ty + rr + M) * G::TW + 4 * tx;  // windows from column xv - 4
+                    const float* rxz = tau + 2 * G::TAU + (ty + rr + M) * G::TW + 4 * tx;
+                    d1[rr] = xderiv1<M, 0>(P, rxx);   // dtxx/dx: txx[i+l-1] - txx[i-l]
+                    d3[rr] = xderiv1<M, 1>(P, rxz);   // dtxz/dx: txz[i+l] - txz[i-l+1]
+                }
+                float4 wz[2 * M + RT - 1], d2[RT], d4[RT];
 #pragma unroll
-                    for (int c4 = 0; c4 < 4; ++c4)
-                        if (!in_stencil(P, xv + c4, j)) {
-                            set_comp(ox, c4, comp(pvx, c4));
-                            set_comp(oz, c4, comp(pvz, c4));
-                        }
+                for (int q = 0; q < 2 * M + RT - 1; ++q)
+                    wz[q] = lds4(tau + 2 * G::TAU + (ty + q) * G::TW + 4 * tx + G::HV);
+                zderivR<M, RT>(P, wz, d2);        // dtxz/dz: txz[j+l-1] - txz[j-l]
+#pragma unroll
+                for (int q = 0; q < 2 * M + RT - 1; ++q)
+                    wz[q] = lds4(tau + G::TAU + (ty + 1 + q) * G::TW + 4 * tx + G::HV);
+                zderivR<M, RT>(P, wz, d4);        // dtzz/dz: tzz[j+l] - tzz[j-l+1]
+#pragma unroll
+                for (int rr = 0; rr < RT; ++rr) {
+                    const int j = vr0 + ty + rr;
+                    ox[rr] = add4(pvx[rr], add4(mul4(pb0[rr], d1[rr]), mul4(pb1[rr], d2[rr])));
+                    oz[rr] = add4(pvz[rr], add4(mul4(pb2[rr], d3[rr]), mul4(pb3[rr], d4[rr])));
+                    if (side || j < M || j > nz - 1 - M) {
+#pragma unroll
+                        for (int c4 = 0; c4 < 4; ++c4)
+                            if (!in_stencil(P, xv + c4, j)) {
+                                set_comp(ox[rr], c4, comp(pvx[rr], c4));
+                                set_comp(oz[rr], c4, comp(pvz[rr], c4));
+                            }
+                    }
                 }
             }
-            const int rr = slot * kMR + ty;    // ring row of grid row j
-            float* rvx = ring + rr * kMVW + 4 * tx;
-            float* rvz = ring + G::RING + rr * kMVW + 4 * tx;
-            *reinterpret_cast<float4*>(rvx) = ox;
-            *reinterpret_cast<float4*>(rvz) = oz;
+            float* rvx = ring + (slot * kMR + ty) * kMVW + 4 * tx;  // ring row of the thread's first row
+            float* rvz = rvx + G::RING;
+#pragma unroll
+            for (int rr = 0; rr < RT; ++rr) {
+                *reinterpret_cast<float4*>(rvx + rr * kMVW) = ox[rr];
+                *reinterpret_cast<float4*>(rvz + rr * kMVW) = oz[rr];
+            }
             const bool band_rows = v_hi > j0 && vr0 <= nz - 2;  // block-uniform
             if (side || band_rows) {
                 __syncthreads();  // pre values of the block in the ring
-                if (side && row_ok && j >= b && j <= j0 - 1) {  // left/right HABC (free surface: rows nbc .. nz-nbc-2)
+                if (side) {  // left/right HABC (free surface: rows nbc .. nz-nbc-2)
                     const SmemRows pre_x{ring, xa, vr0, slot * kMR, G::RING_ROWS, kMVW};
                     const SmemRows pre_z{ring + G::RING, xa, vr0, slot * kMR, G::RING_ROWS, kMVW};
                     const HabcPoint<SmemRows> hx{P, pre_x, P.in[VX], P.w_tab[0]};
                     const HabcPoint<SmemRows> hz{P, pre_z, P.in[VZ], P.w_tab[1]};
 #pragma unroll
-                    for (int c4 = 0; c4 < 4; ++c4) {
-                        const int i = xv + c4;
-                        // the rule's neighbours (left: i+1; right: i-1, i-2) lie in the strip's
-                        // columns for every cell the stress reads (march_plan checks it)
-                        if (lr_band_cell(P, i, j) && (i <= b ? i + 1 < xa + kMVW : i - 2 >= xa)) {
-                            set_comp(ox, c4, hx.final_value(i, j));
-                            set_comp(oz, c4, hz.final_value(i, j));
+                    for (int rr = 0; rr < RT; ++rr) {
+                        const int j = vr0 + ty + rr;
+                        if (!row_ok[rr] || j < b || j > j0 - 1) continue;
+#pragma unroll
+                        for (int c4 = 0; c4 < 4; ++c4) {
+                            const int i = xv + c4;
+                            // the rule's neighbours (left: i+1; right: i-1, i-2) lie in the strip's
+                            // columns for every cell the stress reads (march_plan checks it)
+                            if (lr_band_cell(P, i, j) && (i <= b ? i + 1 < xa + kMVW : i - 2 >= xa)) {
+                                set_comp(ox[rr], c4, hx.final_value(i, j));
+                                set_comp(oz[rr], c4, hz.final_value(i, j));
+                            }
                         }
                     }
                 }
                 __syncthreads();
-                *reinterpret_cast<float4*>(rvx) = ox;
-                *reinterpret_cast<float4*>(rvz) = oz;
+#pragma unroll
+                for (int rr = 0; rr < RT; ++rr) {
+                    *reinterpret_cast<float4*>(rvx + rr * kMVW) = ox[rr];
+                    *reinterpret_cast<float4*>(rvz + rr * kMVW) = oz[rr];
+                }
                 if (band_rows) {
                     __syncthreads();
-                    if (warp < kMarchWarps) {  // all kMarchWarps warps take the march's named barrier
-                        const int f = warp / 3, ws = warp % 3;
-                        march_band_rows(P, w_table(P, f), in_field(P, VX + f), out_field(P, VX + f),
-                                        ring + f * G::RING, kMVW, xa, vr0, slot * kMR, G::RING_ROWS, xa,
-                                        xa + kMVW, x0, x_end, xa + 28 * ws, max(vr0, j0), min(v_hi, nz - 1),
-                                        nullptr);
-                    }
+                    // one round per field, one warp per 28-column strip
+                    for (int f = 0; f < 2; ++f)
+                        if (warp < 3)
+                            march_band_rows(P, w_table(P, f), in_field(P, VX + f), out_field(P, VX + f),
+                                            ring + f * G::RING, kMVW, xa, vr0, slot * kMR, G::RING_ROWS, xa,
+                                            xa + kMVW, x0, x_end, xa + 28 * warp, max(vr0, j0), min(v_hi, nz - 1),
+                                            nullptr, 3);
                     __syncthreads();
-                    ox = *reinterpret_cast<const float4*>(rvx);
-                    oz = *reinterpret_cast<const float4*>(rvz);
+#pragma unroll
+                    for (int rr = 0; rr < RT; ++rr) {
+                        ox[rr] = *reinterpret_cast<const float4*>(rvx + rr * kMVW);
+                        oz[rr] = *reinterpret_cast<const float4*>(rvz + rr * kMVW);
+                    }
                 }
             }
-            if (slot == 0 && ty < 2 * M) {  // the mirror of the ring's first rows
-                *reinterpret_cast<float4*>(rvx + G::RING_ROWS * kMVW) = ox;
-                *reinterpret_cast<float4*>(rvz + G::RING_ROWS * kMVW) = oz;
-            }
-            // the segment's own rows (the rows above are the previous segment's); band rows were
-            // stored by the march
-            if (row_ok && v_own && j >= za && j < zb && !(j >= j0 && j <= nz - 2)) {
-                stg4(P.out[VX] + (xv + j * P.pitch), ox);
-                stg4(P.out[VZ] + (xv + j * P.pitch), oz);
+#pragma unroll
+            for (int rr = 0; rr < RT; ++rr) {
+                const int j = vr0 + ty + rr;
+                if (slot == 0 && ty + rr < 2 * M) {  // the mirror of the ring's first rows
+                    *reinterpret_cast<float4*>(rvx + (rr + G::RING_ROWS) * kMVW) = ox[rr];
+                    *reinterpret_cast<float4*>(rvz + (rr + G::RING_ROWS) * kMVW) = oz[rr];
+                }
+                // the segment's own rows (the rows above are the previous segment's); band rows were
+                // stored by the march
+                if (row_ok[rr] && v_own && j >= za && j < zb && !(j >= j0 && j <= nz - 2)) {
+                    stg4(P.out[VX] + (xv + j * pitch), ox[rr]);
+                    stg4(P.out[VZ] + (xv + j * pitch), oz[rr]);
+                }
             }
         }
         // velocity block t in the ring; every thread is done with iteration t-1.  Thread 0
         // waits for the next iteration's tau boxes here, so the other threads sleep in the
-        // barrier instead of polling.
-        // The flag alternates between two words, so a thread that reads it late still reads the
-        // word written before this barrier (thread 0 rewrites it only two barriers later).
+        // barrier instead of polling.  The flag alternates between two words, so a thread
+        // that reads it late still reads the word written before this barrier (thread 0
+        // rewrites it only two barriers later).
         if (threadIdx.x == 0)
             s_err[(t + 1) & 1] =
                 t + 1 < n_it && !mbar_wait_parity(full + (gt + 1) % kMStages, ((gt + 1) / kMStages) & 1, A.status);
@@ -491,41 +560,54 @@ __device__ __forceinline__ bool march_item(const StepParams& P, const MarchArgs&
         if (t + 1 < n_it) load_v(t + 1);  // velocity block t is done with the current ones
         // ------------------------------------------------ stress block t-1
         if (t >= 1) {
-            const int j = js;
             const float* told = stage + ((gt - 1) % kMStages) * G::STAGE;  // stage t-1: rows from sr0 - 2M
-            const bool row_ok = s_row;
-            float4 oxx = make_float4(0.f, 0.f, 0.f, 0.f), ozz = oxx, oxz = oxx;
-            if (row_ok && s_in) {
-                const int bo = (ty + 2 * M) * G::TW + 2 * G::HV + 4 * tx;
-                const float4 txx = lds4(told + bo), tzz = lds4(told + G::TAU + bo);
-                const float4 txz = lds4(told + 2 * G::TAU + bo);
-                // ring row of grid row j - M + q: r + q
+            float4 oxx[RT], ozz[RT], oxz[RT];
+            bool any = false;
+#pragma unroll
+            for (int rr = 0; rr < RT; ++rr) {
+                oxx[rr] = ozz[rr] = oxz[rr] = make_float4(0.f, 0.f, 0.f, 0.f);
+                any = any || s_row[rr];
+            }
+            if (any && s_in) {
+                float4 txx[RT], tzz[RT], txz[RT], dxx[RT], dzx[RT];
+                // ring row of grid row j - M + q for the thread's first row j: r + q (rows past the
+                // ring are its mirror)
                 const int r = ((t - 1) % kMRing) * kMR + ty;
-                const float* rvx = ring + 4 * tx;
-                const float* rvz = ring + G::RING + 4 * tx;
-                auto rrow = [&](int q) { return (r + q) * kMVW; };  // rows past the ring are its mirror
-                const float4 dxx = xderiv1<M, 1>(P, rvx + rrow(M));  // vx[i+l] - vx[i-l+1]
-                const float4 dzx = xderiv1<M, 0>(P, rvz + rrow(M));  // vz[i+l-1] - vz[i-l]
-                float4 wz[2 * M];
+                const float* rvx = ring + r * kMVW + 4 * tx;
+                const float* rvz = rvx + G::RING;
 #pragma unroll
-                for (int q = 0; q < 2 * M; ++q) wz[q] = lds4(rvz + rrow(q) + G::HV);
-                const float4 dzz = zderiv1<M>(P, wz);       // vz[j+l-1] - vz[j-l]
+                for (int rr = 0; rr < RT; ++rr) {
+                    const int bo = (ty + rr + 2 * M) * G::TW + 2 * G::HV + 4 * tx;
+                    txx[rr] = lds4(told + bo);
+                    tzz[rr] = lds4(told + G::TAU + bo);
+                    txz[rr] = lds4(told + 2 * G::TAU + bo);
+                    dxx[rr] = xderiv1<M, 1>(P, rvx + (rr + M) * kMVW);  // vx[i+l] - vx[i-l+1]
+                    dzx[rr] = xderiv1<M, 0>(P, rvz + (rr + M) * kMVW);  // vz[i+l-1] - vz[i-l]
+                }
+                float4 wz[2 * M + RT - 1], dzz[RT], dxz[RT];
 #pragma unroll
-                for (int q = 0; q < 2 * M; ++q) wz[q] = lds4(rvx + rrow(q + 1) + G::HV);
-                const float4 dxz = zderiv1<M>(P, wz);       // vx[j+l] - vx[j-l+1]
-                const float4 l2m = add4(mlam, mul4s(mmu, 2.f));
-                const float4 ex = mul4s(dxx, P.dtx), ez = mul4s(dzz, P.dtz);
-                oxx = add4(txx, add4(mul4(l2m, ex), mul4(mlam, ez)));
-                ozz = add4(tzz, add4(mul4(mlam, ex), mul4(l2m, ez)));
-                oxz = add4(txz, mul4(mmxz, add4(mul4s(dxz, P.dtz), mul4s(dzx, P.dtx))));
-                if (side || j < M || j > nz - 1 - M) {
+                for (int q = 0; q < 2 * M + RT - 1; ++q) wz[q] = lds4(rvz + q * kMVW + G::HV);
+                zderivR<M, RT>(P, wz, dzz);       // vz[j+l-1] - vz[j-l]
 #pragma unroll
-                    for (int c4 = 0; c4 < 4; ++c4)
-                        if (!in_stencil(P, xs + c4, j)) {
-                            set_comp(oxx, c4, comp(txx, c4));
-                            set_comp(ozz, c4, comp(tzz, c4));
-                            set_comp(oxz, c4, comp(txz, c4));
-                        }
+                for (int q = 0; q < 2 * M + RT - 1; ++q) wz[q] = lds4(rvx + (q + 1) * kMVW + G::HV);
+                zderivR<M, RT>(P, wz, dxz);       // vx[j+l] - vx[j-l+1]
+#pragma unroll
+                for (int rr = 0; rr < RT; ++rr) {
+                    const int j = sr0 + ty + rr;
+                    const float4 l2m = add4(mlam[rr], mul4s(mmu[rr], 2.f));
+                    const float4 ex = mul4s(dxx[rr], P.dtx), ez = mul4s(dzz[rr], P.dtz);
+                    oxx[rr] = add4(txx[rr], add4(mul4(l2m, ex), mul4(mlam[rr], ez)));
+                    ozz[rr] = add4(tzz[rr], add4(mul4(mlam[rr], ex), mul4(l2m, ez)));
+                    oxz[rr] = add4(txz[rr], mul4(mmxz[rr], add4(mul4s(dxz[rr], P.dtz), mul4s(dzx[rr], P.dtx))));
+                    if (side || j < M || j > nz - 1 - M) {
+#pragma unroll
+                        for (int c4 = 0; c4 < 4; ++c4)
+                            if (!in_stencil(P, xs + c4, j)) {
+                                set_comp(oxx[rr], c4, comp(txx[rr], c4));
+                                set_comp(ozz[rr], c4, comp(tzz[rr], c4));
+                                set_comp(oxz[rr], c4, comp(txz[rr], c4));
+                            }
+                    }
                 }
             }
             const bool band_rows = sr0 + kMR > j0 && sr0 <= nz - 2 && sr0 < zb;  // block-uniform
@@ -533,13 +615,17 @@ __device__ __forceinline__ bool march_item(const StepParams& P, const MarchArgs&
                 // exchange through the slot of stage t-1 once every thread has read it
                 __syncthreads();
                 float* sp = stage + ((gt - 1) % kMStages) * G::STAGE;  // [3][16][64], column 0 = x0
+                float* sq = sp + ty * kMVW + 4 * tx;
                 if (s_col) {
-                    *reinterpret_cast<float4*>(sp + ty * kMVW + 4 * tx) = oxx;
-                    *reinterpret_cast<float4*>(sp + kMR * kMVW + ty * kMVW + 4 * tx) = ozz;
-                    *reinterpret_cast<float4*>(sp + 2 * kMR * kMVW + ty * kMVW + 4 * tx) = oxz;
+#pragma unroll
+                    for (int rr = 0; rr < RT; ++rr) {
+                        *reinterpret_cast<float4*>(sq + rr * kMVW) = oxx[rr];
+                        *reinterpret_cast<float4*>(sq + kMR * kMVW + rr * kMVW) = ozz[rr];
+                        *reinterpret_cast<float4*>(sq + 2 * kMR * kMVW + rr * kMVW) = oxz[rr];
+                    }
                 }
                 __syncthreads();
-                if (side && row_ok && s_in && j >= b && j <= j0 - 1) {
+                if (side && s_in) {
                     const SmemRows p0{sp, x0, sr0, 0, kMR, kMVW};
                     const SmemRows p1{sp + kMR * kMVW, x0, sr0, 0, kMR, kMVW};
                     const SmemRows p2{sp + 2 * kMR * kMVW, x0, sr0, 0, kMR, kMVW};
@@ -547,52 +633,67 @@ __device__ __forceinline__ bool march_item(const StepParams& P, const MarchArgs&
                     const HabcPoint<SmemRows> h1{P, p1, P.in[TZZ], P.w_tab[2]};
                     const HabcPoint<SmemRows> h2{P, p2, P.in[TXZ], P.w_tab[2]};
 #pragma unroll
-                    for (int c4 = 0; c4 < 4; ++c4) {
-                        const int i = xs + c4;
-                        if (lr_band_cell(P, i, j) && (i <= b ? i + 1 < x0 + G::W : i - 2 >= x0)) {
-                            set_comp(oxx, c4, h0.final_value(i, j));
-                            set_comp(ozz, c4, h1.final_value(i, j));
-                            set_comp(oxz, c4, h2.final_value(i, j));
+                    for (int rr = 0; rr < RT; ++rr) {
+                        const int j = sr0 + ty + rr;
+                        if (!s_row[rr] || j < b || j > j0 - 1) continue;
+#pragma unroll
+                        for (int c4 = 0; c4 < 4; ++c4) {
+                            const int i = xs + c4;
+                            if (lr_band_cell(P, i, j) && (i <= b ? i + 1 < x0 + G::W : i - 2 >= x0)) {
+                                set_comp(oxx[rr], c4, h0.final_value(i, j));
+                                set_comp(ozz[rr], c4, h1.final_value(i, j));
+                                set_comp(oxz[rr], c4, h2.final_value(i, j));
+                            }
                         }
                     }
                 }
                 __syncthreads();
                 if (s_col) {
-                    *reinterpret_cast<float4*>(sp + ty * kMVW + 4 * tx) = oxx;
-                    *reinterpret_cast<float4*>(sp + kMR * kMVW + ty * kMVW + 4 * tx) = ozz;
-                    *reinterpret_cast<float4*>(sp + 2 * kMR * kMVW + ty * kMVW + 4 * tx) = oxz;
+#pragma unroll
+                    for (int rr = 0; rr < RT; ++rr) {
+                        *reinterpret_cast<float4*>(sq + rr * kMVW) = oxx[rr];
+                        *reinterpret_cast<float4*>(sq + kMR * kMVW + rr * kMVW) = ozz[rr];
+                        *reinterpret_cast<float4*>(sq + 2 * kMR * kMVW + rr * kMVW) = oxz[rr];
+                    }
                 }
                 if (band_rows) {
                     const int ja = max(sr0, j0), jb = min(min(sr0 + kMR, nz - 1), zb);
                     __syncthreads();
-                    if (warp < kMarchWarps) {  // all kMarchWarps warps take the march's named barrier
-                        const int f = warp / 2, ws = warp % 2;
-                        // the row above the first band row: in this block, or the previous block's last row
-                        march_band_rows(P, P.w_tab[2], in_field(P, TXX + f), out_field(P, TXX + f),
-                                        sp + f * kMR * kMVW, kMVW, x0, sr0, 0, kMR, x0, x0 + G::W, x0, x_end,
-                                        x0 + 28 * ws, ja, jb, ja == sr0 ? s_last + f * kMVW : nullptr);
-                    }
+                    // one round per field, one warp per 28-column strip; the row above the first
+                    // band row is in this block, or the previous block's last row
+                    for (int f = 0; f < 3; ++f)
+                        if (warp < 2)
+                            march_band_rows(P, P.w_tab[2], in_field(P, TXX + f), out_field(P, TXX + f),
+                                            sp + f * kMR * kMVW, kMVW, x0, sr0, 0, kMR, x0, x0 + G::W, x0, x_end,
+                                            x0 + 28 * warp, ja, jb, ja == sr0 ? s_last + f * kMVW : nullptr, 2);
                     __syncthreads();
                     if (s_col) {
-                        oxx = *reinterpret_cast<const float4*>(sp + ty * kMVW + 4 * tx);
-                        ozz = *reinterpret_cast<const float4*>(sp + kMR * kMVW + ty * kMVW + 4 * tx);
-                        oxz = *reinterpret_cast<const float4*>(sp + 2 * kMR * kMVW + ty * kMVW + 4 * tx);
+#pragma unroll
+                        for (int rr = 0; rr < RT; ++rr) {
+                            oxx[rr] = *reinterpret_cast<const float4*>(sq + rr * kMVW);
+                            ozz[rr] = *reinterpret_cast<const float4*>(sq + kMR * kMVW + rr * kMVW);
+                            oxz[rr] = *reinterpret_cast<const float4*>(sq + 2 * kMR * kMVW + rr * kMVW);
+                        }
                     }
                 }
             }
-            if (ty == kMR - 1 && s_col) {  // the block's last row, read by the next block's band march
-                *reinterpret_cast<float4*>(s_last + 4 * tx) = oxx;
-                *reinterpret_cast<float4*>(s_last + kMVW + 4 * tx) = ozz;
-                *reinterpret_cast<float4*>(s_last + 2 * kMVW + 4 * tx) = oxz;
+            if (ty + RT == kMR && s_col) {  // the block's last row, read by the next block's band march
+                *reinterpret_cast<float4*>(s_last + 4 * tx) = oxx[RT - 1];
+                *reinterpret_cast<float4*>(s_last + kMVW + 4 * tx) = ozz[RT - 1];
+                *reinterpret_cast<float4*>(s_last + 2 * kMVW + 4 * tx) = oxz[RT - 1];
             }
-            if (row_ok && s_own && !(j >= j0 && j <= nz - 2)) {  // band rows were stored by the march
-                if (in_free_surface_rows(P, j)) {
-                    ozz = make_float4(0.f, 0.f, 0.f, 0.f);
-                    oxz = ozz;
+#pragma unroll
+            for (int rr = 0; rr < RT; ++rr) {
+                const int j = sr0 + ty + rr;
+                if (s_row[rr] && s_own && !(j >= j0 && j <= nz - 2)) {  // band rows were stored by the march
+                    if (in_free_surface_rows(P, j)) {
+                        ozz[rr] = make_float4(0.f, 0.f, 0.f, 0.f);
+                        oxz[rr] = ozz[rr];
+                    }
+                    stg4(P.out[TXX] + (xs + j * pitch), oxx[rr]);
+                    stg4(P.out[TZZ] + (xs + j * pitch), ozz[rr]);
+                    stg4(P.out[TXZ] + (xs + j * pitch), oxz[rr]);
                 }
-                stg4(P.out[TXX] + (xs + j * P.pitch), oxx);
-                stg4(P.out[TZZ] + (xs + j * P.pitch), ozz);
-                stg4(P.out[TXZ] + (xs + j * P.pitch), oxz);
             }
         }
     }

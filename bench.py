@@ -688,6 +688,7 @@ def b200_arm(args, rank, world, local):
                        "shots_per_gpu_per_step": 1, "parallelism": f"shot-sharded x{world}",
                        "l2": "inputs larger than L2 (357 MB medium + 715 MB state per shot)",
                        "step_kernel": args.step_kernel,
+                       "step_kernel_used": "fused" if launches <= args.steps * (w.nt + 1) else "split",
                        "bytes_per_cell_step_algorithmic": 60},
             "physical_cells": {"cells": w.nx_in * w.nz_in,
                                "value": value * (w.nx_in * w.nz_in) / cells,

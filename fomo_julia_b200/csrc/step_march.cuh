@@ -46,7 +46,7 @@ namespace fomo {
 
 constexpr int kMR = 16;            // rows per block
 constexpr int kMVW = 64;           // velocity columns of a strip, halo included
-constexpr int kMRowsPerThread = 2;  // rows of a 16-row block each thread updates (4 columns each)
+constexpr int kMRowsPerThread = 1;  // rows of a 16-row block each thread updates (4 columns each; 2 measured slower)
 constexpr int kMThreads = 16 * kMR / kMRowsPerThread;  // 16 column groups x 16 rows
 constexpr int kMStages = 4;        // tau box stages
 constexpr int kMRing = 3;          // velocity blocks kept

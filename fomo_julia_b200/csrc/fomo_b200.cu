@@ -627,6 +627,42 @@ std::mutex g_step_choice_mu;
 std::map<StepKey, int> g_step_choice;
 constexpr int kStepTuneWindow = 24;  // steps timed per candidate
 
+// The autotuners' optional cache file (environment variable
+// FOMO_B200_TUNE_CACHE).  Single-shot kernel choices are lines
+// "step nx nz M nbc fs iso choice", read on first use and appended to when a
+// choice is made; the shot server's lines have five numbers (server.cuh).
+const char* tune_cache_path() {
+    const char* p = std::getenv("FOMO_B200_TUNE_CACHE");
+    return (p && *p) ? p : nullptr;
+}
+
+// Call with g_step_choice_mu held.
+void load_step_choices() {
+    static bool loaded = false;
+    if (loaded) return;
+    loaded = true;
+    const char* path = tune_cache_path();
+    if (!path) return;
+    FILE* f = std::fopen(path, "r");
+    if (!f) return;
+    char line[256];
+    StepKey k;
+    int c;
+    while (std::fgets(line, sizeof(line), f))
+        if (std::sscanf(line, "step %d %d %d %d %d %d %d", &k.nx, &k.nz, &k.M, &k.nbc, &k.fs, &k.iso, &c) == 7)
+            g_step_choice[k] = c != 0;
+    std::fclose(f);
+}
+
+void save_step_choice(const StepKey& k, int c) {
+    const char* path = tune_cache_path();
+    if (!path) return;
+    if (FILE* f = std::fopen(path, "a")) {
+        std::fprintf(f, "step %d %d %d %d %d %d %d\n", k.nx, k.nz, k.M, k.nbc, k.fs, k.iso, c);
+        std::fclose(f);
+    }
+}
+
 template <int M>
 int run_steps_M(Shot& s, Medium& m, Wavefield& w, int n_steps, Profile* prof) {
     const int mode = g_step_mode.load();
@@ -640,6 +676,7 @@ int run_steps_M(Shot& s, Medium& m, Wavefield& w, int n_steps, Profile* prof) {
         int choice = mode == FOMO_STEP_FUSED ? 1 : -1;
         if (choice < 0) {
             std::lock_guard<std::mutex> lk(g_step_choice_mu);
+            load_step_choices();
             auto it = g_step_choice.find(key);
             if (it != g_step_choice.end()) choice = it->second;
         }
@@ -658,6 +695,7 @@ int run_steps_M(Shot& s, Medium& m, Wavefield& w, int n_steps, Profile* prof) {
                 n_steps -= 2 * W;
                 std::lock_guard<std::mutex> lk(g_step_choice_mu);
                 g_step_choice[key] = choice;
+                save_step_choice(key, choice);
             }
         }
         if (choice == 1) return run_steps_march<M>(s, m, w, n_steps, prof, plan);

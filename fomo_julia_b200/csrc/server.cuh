@@ -146,23 +146,22 @@ struct TuneEntry {
 std::mutex g_tune_mu;
 std::map<TuneKey, TuneEntry> g_tune;  // process-wide cache: (grid, order, batch size) -> K
 
-// Optional file behind the cache (environment variable FOMO_B200_TUNE_CACHE):
-// one line "nx nz M shots_log2 K" per decision, read when a server starts and
-// appended to when a choice is made.  Call with g_tune_mu held.
-const char* tune_cache_path() {
-    const char* p = std::getenv("FOMO_B200_TUNE_CACHE");
-    return (p && *p) ? p : nullptr;
-}
-
+// Optional file behind the cache (environment variable FOMO_B200_TUNE_CACHE,
+// tune_cache_path): one line "nx nz M shots_log2 K" per decision, read when a
+// server starts and appended to when a choice is made (lines of the
+// single-shot kernel choice, "step ...", are skipped here).  Call with
+// g_tune_mu held.
 void load_tune_cache() {
     const char* path = tune_cache_path();
     if (!path) return;
     FILE* f = std::fopen(path, "r");
     if (!f) return;
+    char line[256];
     int nx, nz, M, lg, K;
-    while (std::fscanf(f, "%d %d %d %d %d", &nx, &nz, &M, &lg, &K) == 5)
-        for (int c = 0; c < 3; ++c)
-            if (kTuneK[c] == K) g_tune[TuneKey{nx, nz, M, lg}].chosen = c;
+    while (std::fgets(line, sizeof(line), f))
+        if (std::sscanf(line, "%d %d %d %d %d", &nx, &nz, &M, &lg, &K) == 5)
+            for (int c = 0; c < 3; ++c)
+                if (kTuneK[c] == K) g_tune[TuneKey{nx, nz, M, lg}].chosen = c;
     std::fclose(f);
 }
 

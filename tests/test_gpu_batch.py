@@ -286,3 +286,24 @@ def test_tune_cache_file(b200, tmp_path, monkeypatch):
     lines = path.read_text().split("\n")
     assert any(l.startswith(f"{S.med.nx} {S.med.nz} 4 1 ") for l in lines), lines
     S.med.release()
+
+
+def test_step_kernel_choice_in_tune_cache_file(b200, tmp_path, monkeypatch):
+    # a grid's first shot times the split launches and the fused step on live steps and
+    # records the faster in the cache file; the shot is the same bits either way
+    path = tmp_path / "tune.txt"
+    path.write_text("101 67 4 0 8\n")  # a server line first: both readers skip the other's lines
+    monkeypatch.setenv("FOMO_B200_TUNE_CACHE", str(path))
+    c = layered(103, 59, seed=9, nbc=7, fd_order=8, nt=120)
+    S = setup(c, b200)
+    g = single(S, source(S, 300.0, 20.0), b200)
+    F.set_step_kernel("split")
+    try:
+        ref = single(S, source(S, 300.0, 20.0), b200)
+    finally:
+        F.set_step_kernel("auto")
+    assert np.array_equal(g, ref)
+    lines = [l.split() for l in path.read_text().split("\n") if l.startswith("step ")]
+    assert [l[1:7] for l in lines] == [[str(S.med.nx), str(S.med.nz), "4", "7", "1", "1"]], lines
+    assert lines[0][7] in ("0", "1")
+    S.med.release()

@@ -116,6 +116,7 @@ SIGNATURES = {
     "fomo_b200_shot_profile": [_U64, _I32, ctypes.POINTER(FomoKernelTime), _I32, ctypes.POINTER(_I32)],
     "fomo_b200_selftest_wait": [_I32, ctypes.POINTER(_I32)],
     "fomo_b200_set_step_kernel": [_I32, _I32],
+    "fomo_b200_shot_save_gather": [_U64, ctypes.c_char_p],
     "fomo_b200_run_shot_noalloc": [_I32, _I32, _I32, _I32, _I32, _P, _P, _P, _P, _P, _I32,
                                    ctypes.POINTER(FomoHabc), ctypes.POINTER(FomoShot), _P, _P],
     "fomo_b200_run_batch": [_U64, ctypes.POINTER(FomoHabc), ctypes.POINTER(FomoShot), _I32,

@@ -9,6 +9,7 @@
 #include <nvtx3/nvToolsExt.h>
 
 #include <algorithm>
+#include <cerrno>
 #include <atomic>
 #include <cstdarg>
 #include <cstdio>
@@ -1244,6 +1245,28 @@ int fomo_b200_shot_advance(uint64_t shot_handle, int32_t n_steps, int32_t* k_don
     if (n_steps < 0) return fail(FOMO_EINVAL, "n_steps=%d < 0", n_steps);
     if (int rc = run_steps(*s, n_steps)) return rc;
     if (k_done) *k_done = s->k_done;
+    return FOMO_OK;
+}
+
+int fomo_b200_shot_save_gather(uint64_t shot_handle, const char* path) {
+    std::lock_guard<std::mutex> lk(ctx().mu);
+    if (int rc = ensure_init()) return rc;
+    Shot* s = get<Shot>(shot_handle);
+    if (!s) return fail(FOMO_EINVAL, "unknown shot handle %llu", (unsigned long long)shot_handle);
+    if (!path) return fail(FOMO_EINVAL, "path is NULL");
+    if (int rc = record_last(*s)) return rc;
+    std::vector<float> host((size_t)s->nt * s->n_rec);
+    if (!host.empty()) {
+        CUDA_TRY(cudaMemcpyAsync(host.data(), s->d_gather, host.size() * sizeof(float), cudaMemcpyDeviceToHost,
+                                 ctx().stream));
+        s->d2h += host.size() * sizeof(float);
+    }
+    CUDA_TRY(cudaStreamSynchronize(ctx().stream));
+    FILE* f = std::fopen(path, "wb");
+    if (!f) return fail(FOMO_EINVAL, "cannot open %s for writing: %s", path, std::strerror(errno));
+    const size_t n = host.empty() ? 0 : std::fwrite(host.data(), sizeof(float), host.size(), f);
+    const int closed = std::fclose(f);
+    if (n != host.size() || closed != 0) return fail(FOMO_EINVAL, "writing %s failed", path);
     return FOMO_OK;
 }
 

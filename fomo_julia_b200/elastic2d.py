@@ -16,6 +16,7 @@ from __future__ import annotations
 
 import ctypes
 import math
+import os
 from dataclasses import dataclass, field
 from fractions import Fraction
 from typing import Callable, List, Optional, Sequence
@@ -559,11 +560,16 @@ def _stats_dict(st: FomoRunStats) -> dict:
 
 def run_shot(b: B200Backend, W: Wavefield, M: Medium, H: HABCConfig, a, src: Source, rec: Receivers,
              params: SimParams, shot_id: int = 1, progress: bool = False,
-             on_step: Optional[Callable] = None, step_chunk: int = 1) -> ShotResult:
+             on_step: Optional[Callable] = None, step_chunk: int = 1,
+             gather_path: Optional[str] = None) -> ShotResult:
     """run_shot! (shot_manager.jl:46-68): reset, run nt steps, return the
     gather on the host.  With `on_step` the loop runs in chunks of
     `step_chunk` steps and calls on_step(W, TimeStepInfo) after each chunk;
-    a False return stops the shot early (time_stepper.jl:112-119)."""
+    a False return stops the shot early (time_stepper.jl:112-119).  With
+    `gather_path` the gather is also written there as save_gather's raw
+    .bin (output.jl:28-33), straight from the device seismogram."""
+    if gather_path is not None and on_step is None:
+        on_step, step_chunk = (lambda W_, info: None), params.nt
     keep: list = []
     hs = _ctypes_habc(H, keep)
     ss = _ctypes_shot(a, params, src, rec, keep)
@@ -584,6 +590,8 @@ def run_shot(b: B200Backend, W: Wavefield, M: Medium, H: HABCConfig, a, src: Sou
                 info = TimeStepInfo(k.value, f32(k.value * params.dt), params.nt)
                 if on_step(W, info) is False:
                     break
+            if gather_path is not None:
+                call("fomo_b200_shot_save_gather", sh.value, os.fsencode(gather_path))
         finally:
             call("fomo_b200_shot_finish", sh.value, gather.ctypes.data if gather.size else None,
                  ctypes.byref(st))

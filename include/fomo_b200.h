@@ -218,6 +218,13 @@ int fomo_b200_shot_begin(uint64_t medium, uint64_t wavefield, const FomoHabc* ha
 int fomo_b200_shot_advance(uint64_t shot_handle, int32_t n_steps, int32_t* k_done);
 int fomo_b200_shot_finish(uint64_t shot_handle, float* gather_out, FomoRunStats* stats);
 
+/* save_gather(result, path; format=:bin) (src/io/output.jl:18-33, _save_bin
+ * :28-33) written straight from the shot's device seismogram: raw Float32,
+ * column-major [nt x n_rec] (host byte order, little-endian on the supported
+ * hosts), no header.  Call between begin and finish; the receivers of the last
+ * step done are recorded first, rows after it are zero. */
+int fomo_b200_shot_save_gather(uint64_t shot_handle, const char* path);
+
 /* Per-kernel timing of a shot's loop (no reference counterpart; used by
  * bench.py for the roofline).  Runs up to n_steps more steps of the shot
  * with CUDA events around every launch and reports, per kernel kind

@@ -18,7 +18,7 @@ TOL = 1e-5
 FIELDS = ("vx", "vz", "txx", "tzz", "txz")
 
 
-def gpu_run(c: Case, b200, on_step=None, step_chunk=1, W=None):
+def gpu_run(c: Case, b200, on_step=None, step_chunk=1, W=None, gather_path=None):
     med = F.init_medium(c.vp, c.vs, c.rho, c.dx, c.dz, c.nbc, c.fd_order, b200, free_surface=c.free_surface)
     H = F.init_habc(med.nx, med.nz, c.nbc, c.dt, c.dx, c.dz, c.v_ref, b200)
     params = F.sim_params(c.dt, c.nt, c.dx, c.dz, c.fd_order)
@@ -28,7 +28,8 @@ def gpu_run(c: Case, b200, on_step=None, step_chunk=1, W=None):
     src = F.Source(F.coord_to_index(c.src_x, med.dx, med.pad), F.coord_to_index(c.src_z, med.dz, med.pad), wav)
     own_w = W is None
     W = W or F.Wavefield(med.nx, med.nz, b200)
-    r = F.run_shot(b200, W, med, H, a, src, rec, params, on_step=on_step, step_chunk=step_chunk)
+    r = F.run_shot(b200, W, med, H, a, src, rec, params, on_step=on_step, step_chunk=step_chunk,
+                   gather_path=gather_path)
     fields = {f: W.field(f) for f in FIELDS}
     if own_w:
         W.release()
@@ -213,6 +214,23 @@ def test_on_step_chunks_and_early_stop(b200, oracle_lib):
     g_orc, f_orc = oracle_run(c, oracle_lib, n_steps=stop_at)
     assert_same(early.gather, g_orc, f_early, f_orc)
     assert not early.gather[stop_at:].any()
+
+
+def test_gather_written_from_device(b200, tmp_path):
+    """save_gather's raw .bin (output.jl:28-33) written by the library from the
+    device seismogram: the file holds the returned gather, column-major
+    little-endian Float32, and equals what save_gather writes from the host."""
+    c = layered(37, 31, seed=51, nbc=6, fd_order=8, nt=90, rec_type="p")
+    dev_path, host_path = tmp_path / "dev.bin", tmp_path / "host.bin"
+    r, _ = gpu_run(c, b200, gather_path=str(dev_path))
+    plain, _ = gpu_run(c, b200)
+    assert np.array_equal(r.gather, plain.gather)
+    F.save_gather(r, str(host_path))
+    assert dev_path.read_bytes() == host_path.read_bytes()
+    nt, n_rec = r.gather.shape
+    assert np.array_equal(F.load_gather(str(dev_path), nt, n_rec), r.gather)
+    with pytest.raises(F._lib.FomoError, match="FOMO_EINVAL.*cannot open"):
+        gpu_run(c, b200, gather_path=str(tmp_path / "missing_dir" / "g.bin"))
 
 
 def test_wavefield_reused_across_shots(b200):

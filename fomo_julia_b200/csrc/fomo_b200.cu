@@ -696,7 +696,8 @@ int run_steps_M(Shot& s, Medium& m, Wavefield& w, int n_steps, Profile* prof) {
     }
     if (choice < 0) {
         const int W = kStepTuneWindow;
-        const int n_cand = plan.ok ? 3 : 2;
+        const bool sweep_ok = 2 * ((m.nz + fomo::kTZ - 1) / fomo::kTZ) <= fomo::kSweepMaxRows;
+        const int n_cand = 1 + (plan.ok ? 1 : 0) + (sweep_ok ? 1 : 0);
         if (prof || std::min(n_steps, s.nt - s.k_done) < (n_cand + 1) * W) {
             choice = kChoiceSplit;  // too few steps to time them all: the split launches, nothing recorded
         } else {
@@ -704,9 +705,11 @@ int run_steps_M(Shot& s, Medium& m, Wavefield& w, int n_steps, Profile* prof) {
             double t0 = s.device_ms;
             if (int rc = run_steps_split<M>(s, m, w, W, nullptr)) return rc;
             t[kChoiceSplit] = s.device_ms - t0;
-            t0 = s.device_ms;
-            if (int rc = run_steps_sweep<M>(s, m, w, W, nullptr)) return rc;
-            t[kChoiceSweep] = s.device_ms - t0;
+            if (sweep_ok) {
+                t0 = s.device_ms;
+                if (int rc = run_steps_sweep<M>(s, m, w, W, nullptr)) return rc;
+                t[kChoiceSweep] = s.device_ms - t0;
+            }
             if constexpr (M <= 4) {
                 if (plan.ok) {
                     t0 = s.device_ms;
@@ -830,10 +833,13 @@ struct SweepPlan {
     bool ok = false;
     std::vector<int4> sched;  // {kind, tile row, first item, items}
     int n_items = 0, band_row0 = 0, n_vband = 0, n_sband = 0;
+    std::vector<uint16_t> rows;  // SweepArgs::rows
+    int n_rec = 0, vb0 = 0, sb0 = 0;
 };
 
-SweepPlan sweep_plan(int nx, int nz, int nbc, int M, int tiles_x, int tiles_z, int rec_blocks, int lag) {
+SweepPlan sweep_plan(int nx, int nz, int nbc, int M, int tiles_x, int tiles_z, int rec_blocks, int lag, int chunk) {
     SweepPlan p;
+    const int n_chunks = (tiles_x + chunk - 1) / chunk;
     const int tz = tiles_z;
     const int n_strips = fomo::band_block_count(nx);
     p.band_row0 = std::min(std::max(nz - nbc - 2, 0) / fomo::kTZ, tz - 1);
@@ -854,13 +860,13 @@ SweepPlan sweep_plan(int nx, int nz, int nbc, int M, int tiles_x, int tiles_z, i
         return vband || !reads_band(r);
     };
     auto queue_s = [&](int r) {
-        add(fomo::kSweepSRow, r, tiles_x);
+        add(fomo::kSweepSRow, r, n_chunks);
         if (r == p.band_row0) add(fomo::kSweepSBand, 0, p.n_sband);
     };
     add(fomo::kSweepRecv, 0, rec_blocks);
     int next_s = tz - 1;
     for (int v = tz - 1; v >= 0; --v) {
-        add(fomo::kSweepVRow, v, tiles_x);
+        add(fomo::kSweepVRow, v, n_chunks);
         v_queued[v] = 1;
         if (v == p.band_row0) {
             add(fomo::kSweepVBand, 0, p.n_vband);
@@ -885,17 +891,30 @@ SweepPlan sweep_plan(int nx, int nz, int nbc, int M, int tiles_x, int tiles_z, i
         }
         if (e.x == fomo::kSweepSBand && seen_s > p.band_row0) return p;
     }
-    p.ok = seen_s == 0 && seen_v == 0;
+    if (seen_s != 0 || seen_v != 0 || 2 * tz > fomo::kSweepMaxRows) return p;
+    // the device's form: row entries in order, the band items' offsets after the receivers
+    for (const int4& e : p.sched) {
+        const int at = e.z - (p.sched[0].x == fomo::kSweepRecv ? p.sched[0].w : 0);
+        if (e.x == fomo::kSweepRecv) p.n_rec = e.w;
+        else if (e.x == fomo::kSweepVBand) p.vb0 = at;
+        else if (e.x == fomo::kSweepSBand) p.sb0 = at;
+        else p.rows.push_back((uint16_t)(e.y | (e.x == fomo::kSweepSRow ? 0x8000 : 0)));
+    }
+    p.ok = true;
     return p;
 }
 
 // Stress rows trail the velocity rows they read by this many tile rows
-// (environment variable FOMO_B200_SWEEP_LAG, 1..64; default 6).
-int sweep_lag() {
-    const char* e = std::getenv("FOMO_B200_SWEEP_LAG");
+// (environment variable FOMO_B200_SWEEP_LAG, 1..64; default 16), and a row
+// item is this many consecutive tiles (FOMO_B200_SWEEP_CHUNK, 1..64;
+// default 4).
+int env_int(const char* name, int lo, int hi, int dflt) {
+    const char* e = std::getenv(name);
     const int v = e ? std::atoi(e) : 0;
-    return v >= 1 && v <= 64 ? v : 6;
+    return v >= lo && v <= hi ? v : dflt;
 }
+int sweep_lag() { return env_int("FOMO_B200_SWEEP_LAG", 1, 64, 16); }
+int sweep_chunk() { return env_int("FOMO_B200_SWEEP_CHUNK", 1, 64, 4); }
 
 template <int M>
 int sweep_slots(size_t smem) {
@@ -931,11 +950,13 @@ int run_steps_sweep(Shot& s, Medium& m, Wavefield& w, int n_steps, Profile* prof
     if (int rc = ensure_buoyancy(m, s.dtx, s.dtz)) return rc;
     if (int rc = make_medium_maps(m)) return rc;
     const int rec_blocks = (s.n_rec + fomo::kThreads - 1) / fomo::kThreads;
-    const SweepPlan plan = sweep_plan(m.nx, m.nz, s.nbc, M, L.tiles_x, L.tiles_z, rec_blocks, sweep_lag());
-    if (!plan.ok) return fail(FOMO_EINVAL, "swept step: the item schedule failed its dependency check");
-    // queue (2 ints, padded to 4), counters (2 tiles_z + 2), then the schedule at a 16-byte boundary
-    const size_t n_ctr = 4 + ((2 * (size_t)L.tiles_z + 2 + 3) / 4) * 4;
-    const size_t bytes = n_ctr * sizeof(int) + plan.sched.size() * sizeof(int4);
+    const int chunk = std::min(sweep_chunk(), L.tiles_x);
+    const SweepPlan plan = sweep_plan(m.nx, m.nz, s.nbc, M, L.tiles_x, L.tiles_z, rec_blocks, sweep_lag(), chunk);
+    if (!plan.ok)
+        return fail(FOMO_EINVAL, "the swept step does not support this grid (%d tile rows; at most %d)", L.tiles_z,
+                    fomo::kSweepMaxRows / 2);
+    // queue (2 ints, padded to 4), then the counters (2 tiles_z + 2)
+    const size_t bytes = (4 + 2 * (size_t)L.tiles_z + 2) * sizeof(int);
     if (s.sweep_bytes < bytes) {
         pool_free(s.d_sweep);
         s.d_sweep = nullptr;
@@ -943,10 +964,8 @@ int run_steps_sweep(Shot& s, Medium& m, Wavefield& w, int n_steps, Profile* prof
         CUDA_TRY(pool_alloc(reinterpret_cast<void**>(&s.d_sweep), bytes));
         s.sweep_bytes = bytes;
     }
-    CUDA_TRY(cudaMemsetAsync(s.d_sweep, 0, n_ctr * sizeof(int), C.stream));
-    CUDA_TRY(cudaMemcpyAsync(s.d_sweep + n_ctr, plan.sched.data(), plan.sched.size() * sizeof(int4),
-                             cudaMemcpyHostToDevice, C.stream));
-    fomo::SweepLaunch SL;
+    CUDA_TRY(cudaMemsetAsync(s.d_sweep, 0, bytes, C.stream));
+    static fomo::SweepLaunch SL;  // about 7 KB: kept off the stack (calls hold the context lock)
     std::memset(&SL, 0, sizeof(SL));
     buoyancy_ptrs(m, SL.T.b);
     SL.T.iso = iso ? 1 : 0;
@@ -959,14 +978,18 @@ int run_steps_sweep(Shot& s, Medium& m, Wavefield& w, int n_steps, Profile* prof
     fomo::SweepArgs& A = SL.S;
     A.queue = s.d_sweep;
     A.done = s.d_sweep + 4;
-    A.sched = reinterpret_cast<const int4*>(s.d_sweep + n_ctr);
-    A.n_entries = (int)plan.sched.size();
     A.n_items = plan.n_items;
+    A.n_rec = plan.n_rec;
+    A.vb0 = plan.vb0;
+    A.sb0 = plan.sb0;
+    std::copy(plan.rows.begin(), plan.rows.end(), A.rows);
     A.tiles_z = L.tiles_z;
     A.band_row0 = plan.band_row0;
     A.n_vband = plan.n_vband;
     A.n_sband = plan.n_sband;
-    A.prefetch_ahead = fomo::prefetch_distance(sm_count());
+    A.chunk = chunk;
+    A.n_chunks = (L.tiles_x + chunk - 1) / chunk;
+    A.prefetch_ahead = std::max(1, fomo::prefetch_distance(sm_count()) / chunk);
     const int grid = std::min(sweep_slots<M>(smem), plan.n_items);
     CUDA_TRY(cudaEventRecord(C.ev0, C.stream));
     const int k_begin = s.k_done + 1, k_end = std::min(s.nt, s.k_done + n_steps);

@@ -55,9 +55,9 @@ def parse():
     p.add_argument("--serve-load", type=float, default=4.0,
                    help="offered load of the serving sample, as a multiple of the sequential plain capacity")
     p.add_argument("--no-uneven", action="store_true", help="skip the uneven-batch section")
-    p.add_argument("--step-kernel", choices=["auto", "split", "sweep", "fused"], default="auto",
-                   help="single-shot time-step kernels: the fastest on the grid, timed on live steps (auto), "
-                        "or one of the three")
+    p.add_argument("--step-kernel", choices=["auto", "split", "fused"], default="auto",
+                   help="single-shot time-step kernels: the faster on the grid, timed on live steps (auto), "
+                        "or one of the two")
     p.add_argument("--segs", type=int, default=0, help="fused step: row segments per column strip (0 = auto)")
     return p.parse_args()
 
@@ -307,7 +307,7 @@ def batched_section(args):
 def step_kernel_used(roofline) -> str:
     """Which time-step form the profiled steps ran (the same the timed shots ran)."""
     names = {k["name"] for k in (roofline or {}).get("kernels", [])}
-    return "sweep" if "swept_step" in names else "fused" if "step" in names else "split"
+    return "fused" if "step" in names else "split"
 
 
 def batched_roofline(shot_cell_steps, device_s, shots_per_pass=12):
@@ -607,7 +607,7 @@ def b200_arm(args, rank, world, local):
     call("fomo_b200_shot_begin", med, wf, ctypes.byref(H), ctypes.byref(S), ctypes.byref(sh))
     kt = (FomoKernelTime * 8)()
     nk = ctypes.c_int32(0)
-    call("fomo_b200_shot_profile", sh.value, min(args.profile_steps, w.nt), kt, 6, ctypes.byref(nk))
+    call("fomo_b200_shot_profile", sh.value, min(args.profile_steps, w.nt), kt, 5, ctypes.byref(nk))
     call("fomo_b200_shot_finish", sh.value, None, None)
     kernels = []
     for i in range(nk.value):

@@ -4,8 +4,7 @@
 
 nvcc cross-compiles without a GPU.  Each translation unit (the runtime and
 the split-launch kernels in fomo_b200.cu, one fused-step kernel per order in
-march_m<M>.cu, one swept-step kernel per order in sweep_m<M>.cu) compiles to
-an object in parallel; the objects link into
+march_m<M>.cu) compiles to an object in parallel; the objects link into
 ``fomo_julia_b200/_lib/libfomo_b200.so``, where the package loads it from.
 """
 from __future__ import annotations
@@ -21,8 +20,7 @@ CSRC = os.path.join(HERE, "csrc")
 OUT_DIR = os.path.join(HERE, "_lib")
 OBJ_DIR = os.path.join(OUT_DIR, "obj")
 LIB = os.path.join(OUT_DIR, "libfomo_b200.so")
-SOURCES = ["fomo_b200.cu", "march_m1.cu", "march_m2.cu", "march_m3.cu", "march_m4.cu",
-           "sweep_m1.cu", "sweep_m2.cu", "sweep_m3.cu", "sweep_m4.cu", "sweep_m5.cu", "sweep_m6.cu"]
+SOURCES = ["fomo_b200.cu", "march_m1.cu", "march_m2.cu", "march_m3.cu", "march_m4.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "--fmad=false", "-Xcompiler", "-fPIC,-O2", "--expt-relaxed-constexpr"]
 

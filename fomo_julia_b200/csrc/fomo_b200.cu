@@ -27,8 +27,6 @@
 #include "step_tiled.cuh"
 #include "march_launch.h"
 #include "step_march.cuh"
-#include "step_sweep.cuh"
-#include "sweep_launch.h"
 
 namespace {
 
@@ -122,8 +120,6 @@ struct Shot : Object {
     float* d_band = nullptr;        // band scratch: kBandPlanes planes of nbc rows x pitch
     int* d_rec = nullptr;           // n_rec linear offsets
     float* d_gather = nullptr;      // nt x n_rec
-    int* d_sweep = nullptr;         // swept step: work queue, completion counters, item schedule
-    size_t sweep_bytes = 0;
     int k_done = 0, recorded = 0;
     double device_ms = 0;
     int64_t launches = 0, h2d = 0, d2h = 0;
@@ -132,7 +128,6 @@ struct Shot : Object {
         pool_free(d_band);
         pool_free(d_rec);
         pool_free(d_gather);
-        pool_free(d_sweep);
     }
 };
 
@@ -386,8 +381,7 @@ void fill_common(fomo::StepParams& P, const Medium& m, const Shot& s) {
 // Per-launch event pairs, filled only by fomo_b200_shot_profile.
 struct Profile {
     std::vector<cudaEvent_t> ev;      // 2 per launch
-    std::vector<int> kind;            // 0 velocity, 1 stress, 2 band (velocity), 3 band (stress), 4 fused step,
-                                      // 5 swept step
+    std::vector<int> kind;            // 0 velocity, 1 stress, 2 band (velocity), 3 band (stress), 4 fused step
     int add(cudaStream_t st, int k) {
         cudaEvent_t a, b;
         if (cudaEventCreate(&a) != cudaSuccess || cudaEventCreate(&b) != cudaSuccess) return -1;
@@ -407,8 +401,6 @@ int check_status() {
     CUDA_TRY(cudaMemcpyAsync(&st, ctx().d_status, sizeof(int), cudaMemcpyDeviceToHost, ctx().stream));
     CUDA_TRY(cudaStreamSynchronize(ctx().stream));
     if (st == fomo::kErrTmaTimeout) return fail(FOMO_ETIMEOUT, "a TMA load of a time-step kernel did not complete");
-    if (st == fomo::kErrDepTimeout)
-        return fail(FOMO_ETIMEOUT, "a swept-step item waited too long for the items it reads");
     if (st) return fail(FOMO_ECUDA, "time-step kernel reported error %d", st);
     return FOMO_OK;
 }
@@ -622,13 +614,10 @@ MarchPlan shot_march_plan(const Shot& s, const Medium& m) {
 
 template <int M>
 int run_steps_split(Shot& s, Medium& m, Wavefield& w, int n_steps, Profile* prof);
-template <int M>
-int run_steps_sweep(Shot& s, Medium& m, Wavefield& w, int n_steps, Profile* prof);
 
 // FOMO_STEP_AUTO's choice per grid and HABC width, made once per process by
-// timing the candidates on live steps of the first shot (they give the same
-// bits, so the shot itself is unaffected).
-constexpr int kChoiceSplit = 0, kChoiceFused = 1, kChoiceSweep = 2;
+// timing both kernels on live steps of the first shot (they give the same
+// bits, so the shot itself is unaffected): 0 = split launches, 1 = fused.
 struct StepKey {
     int nx, nz, M, nbc, fs, iso;
     bool operator<(const StepKey& o) const {
@@ -662,7 +651,7 @@ void load_step_choices() {
     int c;
     while (std::fgets(line, sizeof(line), f))
         if (std::sscanf(line, "step %d %d %d %d %d %d %d", &k.nx, &k.nz, &k.M, &k.nbc, &k.fs, &k.iso, &c) == 7)
-            if (c >= kChoiceSplit && c <= kChoiceSweep) g_step_choice[k] = c;
+            g_step_choice[k] = c != 0;
     std::fclose(f);
 }
 
@@ -678,57 +667,39 @@ void save_step_choice(const StepKey& k, int c) {
 template <int M>
 int run_steps_M(Shot& s, Medium& m, Wavefield& w, int n_steps, Profile* prof) {
     const int mode = g_step_mode.load();
-    if (mode == FOMO_STEP_SPLIT) return run_steps_split<M>(s, m, w, n_steps, prof);
-    if (mode == FOMO_STEP_SWEEP) return run_steps_sweep<M>(s, m, w, n_steps, prof);
     const MarchPlan plan = shot_march_plan<M>(s, m);
-    if (mode == FOMO_STEP_FUSED) {
-        if (!plan.ok) return fail(FOMO_EINVAL, "the fused step does not support this shot: %s", plan.why);
-        if constexpr (M <= 4) return run_steps_march<M>(s, m, w, n_steps, prof, plan);
+    if (!plan.ok) {
+        if (mode == FOMO_STEP_FUSED) return fail(FOMO_EINVAL, "the fused step does not support this shot: %s", plan.why);
+        return run_steps_split<M>(s, m, w, n_steps, prof);
     }
-    // FOMO_STEP_AUTO: the recorded choice, or time the candidates on live steps
-    const StepKey key{m.nx, m.nz, M, s.nbc, m.fs, s.dtx == s.dtz};
-    int choice = -1;
-    {
-        std::lock_guard<std::mutex> lk(g_step_choice_mu);
-        load_step_choices();
-        auto it = g_step_choice.find(key);
-        if (it != g_step_choice.end()) choice = it->second;
-    }
-    if (choice < 0) {
-        const int W = kStepTuneWindow;
-        const bool sweep_ok = 2 * ((m.nz + fomo::kTZ - 1) / fomo::kTZ) <= fomo::kSweepMaxRows;
-        const int n_cand = 1 + (plan.ok ? 1 : 0) + (sweep_ok ? 1 : 0);
-        if (prof || std::min(n_steps, s.nt - s.k_done) < (n_cand + 1) * W) {
-            choice = kChoiceSplit;  // too few steps to time them all: the split launches, nothing recorded
-        } else {
-            double t[3] = {1e30, 1e30, 1e30};  // split, fused, swept
-            double t0 = s.device_ms;
-            if (int rc = run_steps_split<M>(s, m, w, W, nullptr)) return rc;
-            t[kChoiceSplit] = s.device_ms - t0;
-            if (sweep_ok) {
-                t0 = s.device_ms;
-                if (int rc = run_steps_sweep<M>(s, m, w, W, nullptr)) return rc;
-                t[kChoiceSweep] = s.device_ms - t0;
-            }
-            if constexpr (M <= 4) {
-                if (plan.ok) {
-                    t0 = s.device_ms;
-                    if (int rc = run_steps_march<M>(s, m, w, W, nullptr, plan)) return rc;
-                    t[kChoiceFused] = s.device_ms - t0;
-                }
-            }
-            choice = kChoiceSplit;
-            for (int c = 1; c < 3; ++c)
-                if (t[c] < t[choice]) choice = c;
-            n_steps -= n_cand * W;
-            std::lock_guard<std::mutex> lk(g_step_choice_mu);
-            g_step_choice[key] = choice;
-            save_step_choice(key, choice);
-        }
-    }
-    if (choice == kChoiceSweep) return run_steps_sweep<M>(s, m, w, n_steps, prof);
     if constexpr (M <= 4) {
-        if (choice == kChoiceFused && plan.ok) return run_steps_march<M>(s, m, w, n_steps, prof, plan);
+        const StepKey key{m.nx, m.nz, M, s.nbc, m.fs, s.dtx == s.dtz};
+        int choice = mode == FOMO_STEP_FUSED ? 1 : -1;
+        if (choice < 0) {
+            std::lock_guard<std::mutex> lk(g_step_choice_mu);
+            load_step_choices();
+            auto it = g_step_choice.find(key);
+            if (it != g_step_choice.end()) choice = it->second;
+        }
+        if (choice < 0) {
+            const int W = kStepTuneWindow;
+            if (prof || std::min(n_steps, s.nt - s.k_done) < 3 * W) {
+                choice = 0;  // too few steps to time both: the split launches, nothing recorded
+            } else {
+                double t0 = s.device_ms;
+                if (int rc = run_steps_march<M>(s, m, w, W, nullptr, plan)) return rc;
+                const double t_fused = s.device_ms - t0;
+                t0 = s.device_ms;
+                if (int rc = run_steps_split<M>(s, m, w, W, nullptr)) return rc;
+                const double t_split = s.device_ms - t0;
+                choice = t_fused < t_split ? 1 : 0;
+                n_steps -= 2 * W;
+                std::lock_guard<std::mutex> lk(g_step_choice_mu);
+                g_step_choice[key] = choice;
+                save_step_choice(key, choice);
+            }
+        }
+        if (choice == 1) return run_steps_march<M>(s, m, w, n_steps, prof, plan);
     }
     return run_steps_split<M>(s, m, w, n_steps, prof);
 }
@@ -809,229 +780,6 @@ int run_steps_split(Shot& s, Medium& m, Wavefield& w, int n_steps, Profile* prof
         fomo::band_kernel<false><<<L.n_band, 32, 0, C.stream>>>(P, T);
         if (prof && prof->end(C.stream)) return fail(FOMO_ECUDA, "profiling event failed");
         s.launches += 4;
-        w.cur = b;
-        if (k >= 2) s.recorded = k - 1;
-        s.k_done = k;
-    }
-    nvtxRangePop();
-    CUDA_TRY(cudaGetLastError());
-    CUDA_TRY(cudaEventRecord(C.ev1, C.stream));
-    CUDA_TRY(cudaEventSynchronize(C.ev1));
-    float ms = 0;
-    CUDA_TRY(cudaEventElapsedTime(&ms, C.ev0, C.ev1));
-    s.device_ms += ms;
-    return check_status();
-}
-
-// ---------------------------------------------------------------- swept step
-// Queue order of the swept step (step_sweep.cuh) on a tiles_x x tiles_z tile
-// grid: receivers, then velocity rows bottom to top, each stress row `lag`
-// rows behind the velocity row it trails, and each band pass right after the
-// last row it reads.  Every item's inputs come from items before it (checked
-// here), so a block never waits for an item no block has taken.
-struct SweepPlan {
-    bool ok = false;
-    std::vector<int4> sched;  // {kind, tile row, first item, items}
-    int n_items = 0, band_row0 = 0, n_vband = 0, n_sband = 0;
-    std::vector<uint16_t> rows;  // SweepArgs::rows
-    int n_rec = 0, vb0 = 0, sb0 = 0;
-};
-
-SweepPlan sweep_plan(int nx, int nz, int nbc, int M, int tiles_x, int tiles_z, int rec_blocks, int lag, int chunk) {
-    SweepPlan p;
-    const int n_chunks = (tiles_x + chunk - 1) / chunk;
-    const int tz = tiles_z;
-    const int n_strips = fomo::band_block_count(nx);
-    p.band_row0 = std::min(std::max(nz - nbc - 2, 0) / fomo::kTZ, tz - 1);
-    p.n_vband = (2 * n_strips + fomo::kBandWarpsPerItem - 1) / fomo::kBandWarpsPerItem;
-    p.n_sband = (3 * n_strips + fomo::kBandWarpsPerItem - 1) / fomo::kBandWarpsPerItem;
-    // the split stress launch's reads_band_rows, per tile row
-    auto reads_band = [&](int r) { return r * fomo::kTZ + fomo::kTZ + fomo::kEdgeZ + M >= nz - nbc - 1; };
-    auto add = [&](int kind, int row, int count) {
-        if (count <= 0) return;
-        p.sched.push_back(make_int4(kind, row, p.n_items, count));
-        p.n_items += count;
-    };
-    std::vector<char> v_queued(tz, 0);
-    bool vband = false;
-    auto s_ready = [&](int r) {
-        for (int q = std::max(r - 1, 0); q <= std::min(r + 1, tz - 1); ++q)
-            if (!v_queued[q]) return false;
-        return vband || !reads_band(r);
-    };
-    auto queue_s = [&](int r) {
-        add(fomo::kSweepSRow, r, n_chunks);
-        if (r == p.band_row0) add(fomo::kSweepSBand, 0, p.n_sband);
-    };
-    add(fomo::kSweepRecv, 0, rec_blocks);
-    int next_s = tz - 1;
-    for (int v = tz - 1; v >= 0; --v) {
-        add(fomo::kSweepVRow, v, n_chunks);
-        v_queued[v] = 1;
-        if (v == p.band_row0) {
-            add(fomo::kSweepVBand, 0, p.n_vband);
-            vband = true;
-        }
-        while (next_s >= 0 && next_s >= v + lag && s_ready(next_s)) queue_s(next_s--);
-    }
-    while (next_s >= 0) queue_s(next_s--);
-    // check: every stress row after the velocity rows and band pass it reads,
-    // each band pass after the rows it reads
-    int seen_v = tz, seen_s = tz;  // lowest velocity / stress row queued so far
-    bool seen_vband = false;
-    for (const int4& e : p.sched) {
-        if (e.x == fomo::kSweepVRow) seen_v = e.y;
-        if (e.x == fomo::kSweepVBand) {
-            if (seen_v > p.band_row0) return p;
-            seen_vband = true;
-        }
-        if (e.x == fomo::kSweepSRow) {
-            if (seen_v > std::max(e.y - 1, 0) || (reads_band(e.y) && !seen_vband)) return p;
-            seen_s = e.y;
-        }
-        if (e.x == fomo::kSweepSBand && seen_s > p.band_row0) return p;
-    }
-    if (seen_s != 0 || seen_v != 0 || 2 * tz > fomo::kSweepMaxRows) return p;
-    // the device's form: row entries in order, the band items' offsets after the receivers
-    for (const int4& e : p.sched) {
-        const int at = e.z - (p.sched[0].x == fomo::kSweepRecv ? p.sched[0].w : 0);
-        if (e.x == fomo::kSweepRecv) p.n_rec = e.w;
-        else if (e.x == fomo::kSweepVBand) p.vb0 = at;
-        else if (e.x == fomo::kSweepSBand) p.sb0 = at;
-        else p.rows.push_back((uint16_t)(e.y | (e.x == fomo::kSweepSRow ? 0x8000 : 0)));
-    }
-    p.ok = true;
-    return p;
-}
-
-// Stress rows trail the velocity rows they read by this many tile rows
-// (environment variable FOMO_B200_SWEEP_LAG, 1..64; default 16), and a row
-// item is this many consecutive tiles (FOMO_B200_SWEEP_CHUNK, 1..64;
-// default 4).
-int env_int(const char* name, int lo, int hi, int dflt) {
-    const char* e = std::getenv(name);
-    const int v = e ? std::atoi(e) : 0;
-    return v >= lo && v <= hi ? v : dflt;
-}
-int sweep_lag() { return env_int("FOMO_B200_SWEEP_LAG", 1, 64, 16); }
-int sweep_chunk() { return env_int("FOMO_B200_SWEEP_CHUNK", 1, 64, 4); }
-
-template <int M>
-int sweep_slots(size_t smem) {
-    static std::mutex mu;
-    static std::map<std::pair<int, size_t>, int> slots;
-    int dev = 0;
-    CUDA_TRY(cudaGetDevice(&dev));
-    std::lock_guard<std::mutex> lk(mu);
-    auto it = slots.find({dev, smem});
-    if (it != slots.end()) return it->second;
-    int per_sm = 0;
-    if (raise_smem_limit(fomo::sweep_kernel_fn<M>(), smem) != FOMO_OK ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fomo::sweep_kernel_fn<M>(), fomo::kThreads, smem) !=
-            cudaSuccess) {
-        (void)cudaGetLastError();
-        per_sm = 1;
-    }
-    const int n = std::max(1, per_sm) * sm_count();
-    slots[{dev, smem}] = n;
-    return n;
-}
-
-// The swept step: one persistent launch per step (step_sweep.cuh).
-template <int M>
-int run_steps_sweep(Shot& s, Medium& m, Wavefield& w, int n_steps, Profile* prof) {
-    auto& C = ctx();
-    const bool iso = s.dtx == s.dtz;
-    const Launch L = launch_shape<M>(m.nx, m.nz, s.nbc, iso, m.fs != 0);
-    const size_t smem = std::max(std::max(L.smem_v, L.smem_s), fomo::sweep_band_smem(s.nbc));
-    if (int rc = raise_smem_limit(fomo::sweep_kernel_fn<M>(), smem)) return rc;
-    if (w.map_M != M)
-        if (int rc = make_maps<M>(w)) return rc;
-    if (int rc = ensure_buoyancy(m, s.dtx, s.dtz)) return rc;
-    if (int rc = make_medium_maps(m)) return rc;
-    const int rec_blocks = (s.n_rec + fomo::kThreads - 1) / fomo::kThreads;
-    const int chunk = std::min(sweep_chunk(), L.tiles_x);
-    const SweepPlan plan = sweep_plan(m.nx, m.nz, s.nbc, M, L.tiles_x, L.tiles_z, rec_blocks, sweep_lag(), chunk);
-    if (!plan.ok)
-        return fail(FOMO_EINVAL, "the swept step does not support this grid (%d tile rows; at most %d)", L.tiles_z,
-                    fomo::kSweepMaxRows / 2);
-    // queue (2 ints, padded to 4), then the counters (2 tiles_z + 2)
-    const size_t bytes = (4 + 2 * (size_t)L.tiles_z + 2) * sizeof(int);
-    if (s.sweep_bytes < bytes) {
-        pool_free(s.d_sweep);
-        s.d_sweep = nullptr;
-        s.sweep_bytes = 0;
-        CUDA_TRY(pool_alloc(reinterpret_cast<void**>(&s.d_sweep), bytes));
-        s.sweep_bytes = bytes;
-    }
-    CUDA_TRY(cudaMemsetAsync(s.d_sweep, 0, bytes, C.stream));
-    static fomo::SweepLaunch SL;  // about 7 KB: kept off the stack (calls hold the context lock)
-    std::memset(&SL, 0, sizeof(SL));
-    buoyancy_ptrs(m, SL.T.b);
-    SL.T.iso = iso ? 1 : 0;
-    SL.T.status = C.d_status;
-    SL.T.band_pre = s.d_band;
-    SL.T.n_tile_blocks = L.n_tile;
-    SL.T.tiles_x = L.tiles_x;
-    SL.T.x_last = L.x_last;
-    SL.T.prefetch_ahead = 0;
-    fomo::SweepArgs& A = SL.S;
-    A.queue = s.d_sweep;
-    A.done = s.d_sweep + 4;
-    A.n_items = plan.n_items;
-    A.n_rec = plan.n_rec;
-    A.vb0 = plan.vb0;
-    A.sb0 = plan.sb0;
-    std::copy(plan.rows.begin(), plan.rows.end(), A.rows);
-    A.tiles_z = L.tiles_z;
-    A.band_row0 = plan.band_row0;
-    A.n_vband = plan.n_vband;
-    A.n_sband = plan.n_sband;
-    A.chunk = chunk;
-    A.n_chunks = (L.tiles_x + chunk - 1) / chunk;
-    A.prefetch_ahead = std::max(1, fomo::prefetch_distance(sm_count()) / chunk);
-    const int grid = std::min(sweep_slots<M>(smem), plan.n_items);
-    CUDA_TRY(cudaEventRecord(C.ev0, C.stream));
-    const int k_begin = s.k_done + 1, k_end = std::min(s.nt, s.k_done + n_steps);
-    nvtxRangePushA("fomo_b200 time loop (swept step)");
-    for (int k = k_begin; k <= k_end; ++k) {
-        const int a = w.cur, b = 1 - w.cur;
-        fomo::StepParams& Pv = SL.Pv;
-        fill_common(Pv, m, s);
-        Pv.src_w = (k <= (int)s.wavelet.size()) ? s.wavelet[k - 1] : 0.f;
-        for (int q = 0; q < 5; ++q) Pv.in[q] = w.field(a, q);
-        Pv.out[fomo::VX] = w.field(b, fomo::VX);
-        Pv.out[fomo::VZ] = w.field(b, fomo::VZ);
-        Pv.rec_k = (k >= 2 && s.n_rec > 0) ? k - 1 : 0;
-        fomo::StepParams& Ps = SL.Ps;
-        Ps = Pv;
-        Ps.in[fomo::VX] = w.field(b, fomo::VX);
-        Ps.in[fomo::VZ] = w.field(b, fomo::VZ);
-        for (int q = 2; q < 5; ++q) Ps.out[q] = w.field(b, q);
-        Ps.out[fomo::VX] = Ps.out[fomo::VZ] = nullptr;
-        Ps.rec_k = 0;
-        SL.vm.xx = w.maps[a][fomo::TXX];
-        SL.vm.zz = w.maps[a][fomo::TZZ];
-        SL.vm.xz = w.maps[a][fomo::TXZ];
-        SL.vm.vx = w.pmaps[a][fomo::VX];
-        SL.vm.vz = w.pmaps[a][fomo::VZ];
-        SL.vm.b0 = m.buoy_maps[0];
-        SL.vm.b1 = m.buoy_maps[1];
-        SL.vm.b2 = m.buoy_maps[2];
-        SL.vm.b3 = m.buoy_maps[3];
-        SL.sm.vx = w.maps[b][fomo::VX];
-        SL.sm.vz = w.maps[b][fomo::VZ];
-        SL.sm.txx = w.pmaps[a][fomo::TXX];
-        SL.sm.tzz = w.pmaps[a][fomo::TZZ];
-        SL.sm.txz = w.pmaps[a][fomo::TXZ];
-        SL.sm.lam = m.mod_maps[0];
-        SL.sm.mu = m.mod_maps[1];
-        SL.sm.mxz = m.mod_maps[2];
-        A.epoch = k - k_begin;
-        if (prof && prof->add(C.stream, 5)) return fail(FOMO_ECUDA, "profiling event failed");
-        CUDA_TRY(fomo::sweep_launch<M>(grid, smem, C.stream, SL));
-        if (prof && prof->end(C.stream)) return fail(FOMO_ECUDA, "profiling event failed");
-        s.launches += 1;
         w.cur = b;
         if (k >= 2) s.recorded = k - 1;
         s.k_done = k;
@@ -1553,7 +1301,7 @@ int fomo_b200_shot_profile(uint64_t shot_handle, int32_t n_steps, FomoKernelTime
     if (!s) return fail(FOMO_EINVAL, "unknown shot handle %llu", (unsigned long long)shot_handle);
     if (n_steps < 0 || n_steps > 100000 || !out || !n_kinds || max_kinds < 4)
         return fail(FOMO_EINVAL, "bad profile arguments (max_kinds must be >= 4)");
-    const int nk = std::min<int>(max_kinds, 6);
+    const int nk = max_kinds >= 5 ? 5 : 4;
     Medium* m = get<Medium>(s->medium);
     if (!m) return fail(FOMO_EINVAL, "shot refers to a destroyed medium");
     Profile prof;
@@ -1567,16 +1315,13 @@ int fomo_b200_shot_profile(uint64_t shot_handle, int32_t n_steps, FomoKernelTime
     // output field and write its final value (24 B/cell velocity, 36 stress).
     // The fused step reads the five fields, two buoyancy arrays (four when
     // dx != dz) and lam, mu_txx, mu_txz, and writes the five fields
-    // (60 B/cell, 68 B with four buoyancy arrays), and so does the swept step
-    // (the tile launches' 80 B/cell less the tau and v re-reads its order
-    // leaves to L2).
+    // (60 B/cell, 68 B with four buoyancy arrays).
     const double cells = (double)m->nx * m->nz, band = (double)s->nbc * m->nx;
-    const double step_bytes = (s->dtx == s->dtz ? 60.0 : 68.0) * cells;
-    const char* names[6] = {"velocity", "stress", "band_velocity", "band_stress", "step", "swept_step"};
-    const double bytes[6] = {36.0 * cells, 44.0 * cells, 24.0 * band, 36.0 * band, step_bytes, step_bytes};
+    const char* names[5] = {"velocity", "stress", "band_velocity", "band_stress", "step"};
+    const double bytes[5] = {36.0 * cells, 44.0 * cells, 24.0 * band, 36.0 * band,
+                             (s->dtx == s->dtz ? 60.0 : 68.0) * cells};
     for (size_t i = 0; i < prof.kind.size(); ++i)
-        if (prof.kind[i] >= nk)
-            return fail(FOMO_EINVAL, "the %s kernel ran: max_kinds must be >= %d", names[prof.kind[i]], prof.kind[i] + 1);
+        if (prof.kind[i] >= nk) return fail(FOMO_EINVAL, "the fused step ran: max_kinds must be >= 5");
     for (int k = 0; k < nk; ++k) {
         std::memset(&out[k], 0, sizeof(FomoKernelTime));
         std::snprintf(out[k].name, sizeof(out[k].name), "%s", names[k]);
@@ -1593,7 +1338,7 @@ int fomo_b200_shot_profile(uint64_t shot_handle, int32_t n_steps, FomoKernelTime
 }
 
 int fomo_b200_set_step_kernel(int32_t mode, int32_t n_segs) {
-    if (mode != FOMO_STEP_AUTO && mode != FOMO_STEP_SPLIT && mode != FOMO_STEP_FUSED && mode != FOMO_STEP_SWEEP)
+    if (mode != FOMO_STEP_AUTO && mode != FOMO_STEP_SPLIT && mode != FOMO_STEP_FUSED)
         return fail(FOMO_EINVAL, "unknown step kernel mode %d", mode);
     if (n_segs < 0 || n_segs > fomo::kMMaxSegs)
         return fail(FOMO_EINVAL, "n_segs=%d out of range 0..%d", n_segs, fomo::kMMaxSegs);

@@ -258,8 +258,7 @@ __device__ void load_region_inputs(const StepParams& P, int xa, int za, int W, i
         const int i = xa - M + xx, j = za - M + zz;
         float v = 0.f;
         if (i >= 0 && i < P.nx && j >= 0 && j < P.nz)
-            // the new v: a plain load (the swept step writes it in the same launch)
-            v = VEL ? tau_in(P, TXX + f, i, j, src_w) : in_field(P, VX + f)[cell(P, i, j)];
+            v = VEL ? tau_in(P, TXX + f, i, j, src_w) : __ldg(in_field(P, VX + f) + cell(P, i, j));
         sin[idx] = v;
     }
 }

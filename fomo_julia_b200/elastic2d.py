@@ -92,20 +92,17 @@ def synchronize(b: B200Backend = B200_BACKEND) -> None:
     call("fomo_b200_synchronize")
 
 
-STEP_KERNELS = {"auto": 0, "split": 1, "fused": 2, "sweep": 3}
+STEP_KERNELS = {"auto": 0, "split": 1, "fused": 2}
 
 
 def set_step_kernel(mode: str = "auto", n_segs: int = 0) -> None:
     """Time-step kernels of single shots (no reference counterpart).  "split":
     four launches per step (velocity tiles, velocity band pass, stress
-    tiles, stress band pass); "sweep": one persistent launch per step over
-    the same tiles, ordered so the stress tiles re-read tau and the new v
-    from L2 (stress rows trail by FOMO_B200_SWEEP_LAG tile rows, default 6);
-    "fused": one launch per step computing velocity and stress in column
-    strips (fails a shot it cannot run); "auto": times the candidates on the
-    first long enough shot of a grid and keeps the fastest.  n_segs > 0 fixes
-    the fused step's row segments per column strip.  Results are the same
-    bit for bit."""
+    tiles, stress band pass); "fused": one launch per step computing velocity
+    and stress in column strips (fails a shot it cannot run); "auto": times
+    both on the first long enough shot of a grid and keeps the faster.
+    n_segs > 0 fixes the fused step's row segments per column strip.  Results
+    are the same bit for bit."""
     call("fomo_b200_set_step_kernel", STEP_KERNELS[mode], int(n_segs))
 
 

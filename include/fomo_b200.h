@@ -228,8 +228,8 @@ int fomo_b200_shot_save_gather(uint64_t shot_handle, const char* path);
 /* Per-kernel timing of a shot's loop (no reference counterpart; used by
  * bench.py for the roofline).  Runs up to n_steps more steps of the shot
  * with CUDA events around every launch and reports, per kernel kind
- * (velocity, stress, band_velocity, band_stress: max_kinds >= 4; step, the
- * fused step, when max_kinds >= 5; swept_step when max_kinds >= 6), the
+ * (velocity, stress, band_velocity, band_stress: max_kinds >= 4; and step,
+ * the fused step, when max_kinds >= 5), the
  * launches, their summed device time and the algorithmic DRAM bytes of one
  * launch (the bytes a launch must move at minimum: each array it reads
  * once and each array it writes once, over the cells it updates). */
@@ -244,31 +244,25 @@ int fomo_b200_shot_profile(uint64_t shot_handle, int32_t n_steps, FomoKernelTime
                            int32_t max_kinds, int32_t* n_kinds);
 
 /* Time-step kernel selection (no reference counterpart; a tuning control).
- * Three forms of the time step give the same bits:
- *   split launches  -- velocity tiles, velocity band pass, stress tiles,
- *                      stress band pass (four launches per step);
- *   swept step      -- one persistent launch per step over the same tiles and
- *                      band passes, ordered so that the stress tiles re-read
- *                      tau and the new v from L2 instead of HBM; stress rows
- *                      trail the velocity rows by FOMO_B200_SWEEP_LAG tile rows
- *                      (environment variable, 1..64, default 6);
- *   fused step      -- one launch per step that computes velocity and stress
- *                      in column strips (free surface, M <= 4, HABC bands that
- *                      fit its first and last strips).
- * FOMO_STEP_AUTO times the candidates on 24 live steps each of the first
- * shot of a (grid, order, HABC width) with enough steps left and keeps the
- * fastest for the process (and in the FOMO_B200_TUNE_CACHE file when that is
- * set); shots too short to time run the split launches.  FOMO_STEP_SPLIT,
- * FOMO_STEP_SWEEP and FOMO_STEP_FUSED force one form; FOMO_STEP_FUSED fails a
- * single shot that the fused step does not support with FOMO_EINVAL.
- * n_segs > 0 fixes the fused step's row segments per column strip (1..64;
- * 0 = chosen from the grid and the SM count).  Process-wide.  The batched and
- * served paths run the fused step under FOMO_STEP_FUSED and the split
- * launches otherwise; fomo_b200_run_shot_noalloc runs the split launches. */
+ * Two forms of the time step give the same bits: the split launches
+ * (velocity tiles, velocity band pass, stress tiles, stress band pass) and
+ * the fused step -- one launch per time step that computes velocity and
+ * stress together in column strips, so every field and medium array crosses
+ * HBM once (free surface, M <= 4, HABC bands that fit its first and last
+ * strips).  FOMO_STEP_AUTO times both on 24 live steps each of the first
+ * shot of a (grid, order, HABC width) with enough steps left, keeps the
+ * faster for the process (and in the FOMO_B200_TUNE_CACHE file when that is
+ * set), and runs the split launches where the fused step does not apply or
+ * the shot is too short to time.  FOMO_STEP_SPLIT always runs the split
+ * launches; FOMO_STEP_FUSED fails a single shot that the fused step does not
+ * support with FOMO_EINVAL.  n_segs > 0 fixes the fused step's row segments
+ * per column strip (1..64; 0 = chosen from the grid and the SM count).
+ * Process-wide.  The batched and served paths run the fused step under
+ * FOMO_STEP_FUSED and the split launches otherwise;
+ * fomo_b200_run_shot_noalloc runs the split launches. */
 #define FOMO_STEP_AUTO 0
 #define FOMO_STEP_SPLIT 1
 #define FOMO_STEP_FUSED 2
-#define FOMO_STEP_SWEEP 3
 int fomo_b200_set_step_kernel(int32_t mode, int32_t n_segs);
 
 /* Self-test of the kernels' bounded device waits (no reference

@@ -149,29 +149,6 @@ def test_fused_step_matches_oracle(c, b200, oracle_lib, step_kernel):
     assert r.stats["kernel_launches"] <= c.nt + 1
 
 
-@pytest.mark.parametrize("c", CASES, ids=lambda c: c.name)
-def test_swept_step_matches_oracle(c, b200, oracle_lib, step_kernel):
-    """The swept step (one persistent launch per step over the split tiles)
-    runs every shot the split launches run, with the same bits."""
-    step_kernel("sweep")
-    r, f_gpu = gpu_run(c, b200)
-    assert r.stats["kernel_launches"] <= c.nt + 1
-    g_orc, f_orc = oracle_run(c, oracle_lib)
-    assert_same(r.gather, g_orc, f_gpu, f_orc)
-
-
-@pytest.mark.parametrize("lag", [1, 2, 64])
-def test_swept_step_lags(lag, b200, oracle_lib, step_kernel, monkeypatch):
-    """Stress rows right behind the velocity rows they read (lag 1, the most
-    dependency waits), and all of them after every velocity row (lag 64)."""
-    monkeypatch.setenv("FOMO_B200_SWEEP_LAG", str(lag))
-    step_kernel("sweep")
-    c = layered(231, 150, seed=23, nbc=10, fd_order=8, nt=70, n_rec=31)
-    r, f_gpu = gpu_run(c, b200)
-    g_orc, f_orc = oracle_run(c, oracle_lib)
-    assert_same(r.gather, g_orc, f_gpu, f_orc)
-
-
 @pytest.mark.parametrize("c", [c for c in CASES if fused_supported(c)], ids=lambda c: c.name)
 def test_split_launches_match_oracle(c, b200, oracle_lib, step_kernel):
     # the same shots through the split launches (velocity, band pass, stress, band pass)

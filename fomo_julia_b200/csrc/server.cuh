@@ -502,7 +502,7 @@ class Server {
     std::vector<LaunchSet> sets_;
     std::vector<MarchSet> msets_;  // fused-step sets (their counters follow the split sets')
     cudaError_t enqueue_err_ = cudaSuccess;
-    std::map<int, cudaGraphExec_t> graphs_;  // K -> graph of the current tables
+    std::map<int, cudaGraphExec_t> graphs_;  // 2K + parity of its first step -> graph of the current tables
     std::deque<cudaEvent_t> inflight_;
     std::vector<Deferred> deferred_;
     std::vector<Measure> measures_;
@@ -947,12 +947,14 @@ class Server {
     // One batch step, set after set.  `after_band`: the last launch on the
     // stream is the previous step's last stress band pass, so the first
     // velocity launch may start beside it (every later tile launch follows
-    // a band pass).
-    void enqueue_step(bool after_band) {
+    // a band pass).  `k`: the batch step (only its parity goes into the
+    // launches, which take it as the copy parity of their shots).
+    void enqueue_step(bool after_band, int64_t k) {
         // the previous step ended with a band pass only without fused-step sets
         after_band = after_band && msets_.empty();
         for (size_t i = 0; i < sets_.size(); ++i) {
             const LaunchSet& S = sets_[i];
+            S.lv->H.kpar = S.ls->H.kpar = (int)(k & 1);
             launch_batch(true, S, st_, after_band || i > 0);
             fomo::batch_band_kernel<true, fomo::BatchVelLaunch><<<S.grid_b, 32, 0, st_>>>(*S.lv);
             launch_batch(false, S, st_, true);
@@ -972,15 +974,17 @@ class Server {
         return FOMO_OK;
     }
 
-    int graph_for(int K, cudaGraphExec_t* out) {
-        auto it = graphs_.find(K);
+    // The graph of K batch steps starting at a step of parity p0.
+    int graph_for(int K, int p0, cudaGraphExec_t* out) {
+        const int key = 2 * K + p0;
+        auto it = graphs_.find(key);
         if (it != graphs_.end()) {
             *out = it->second;
             return FOMO_OK;
         }
         cudaGraph_t g = nullptr;
         CUDA_TRY(cudaStreamBeginCapture(st_, cudaStreamCaptureModeThreadLocal));
-        for (int k = 0; k < K; ++k) enqueue_step(k > 0);
+        for (int k = 0; k < K; ++k) enqueue_step(k > 0, p0 + k);
         cudaError_t e = cudaStreamEndCapture(st_, &g);
         if (int rc = take_enqueue_error()) {
             if (g) cudaGraphDestroy(g);
@@ -994,7 +998,7 @@ class Server {
         // upload now, so the first replay (maybe a timed one) does not carry it
         e = cudaGraphUpload(x, st_);
         if (e != cudaSuccess) return fail(FOMO_ECUDA, "graph upload failed: %s", cudaGetErrorString(e));
-        graphs_[K] = x;
+        graphs_[key] = x;
         *out = x;
         return FOMO_OK;
     }
@@ -1080,7 +1084,7 @@ class Server {
         if (n != chunk) measure = false;
         cudaGraphExec_t x = nullptr;
         if (graph)
-            if (int rc = graph_for(K, &x)) return rc;
+            if (int rc = graph_for(K, (int)((k_host_ + 1) & 1), &x)) return rc;
         Measure ms{};
         if (measure) {
             double cells = 0;
@@ -1098,7 +1102,7 @@ class Server {
             nvtxRangePop();
             CUDA_TRY(e);
         } else {
-            for (int k = 0; k < n; ++k) enqueue_step(k > 0);
+            for (int k = 0; k < n; ++k) enqueue_step(k > 0, k_host_ + 1 + k);
             nvtxRangePop();
             CUDA_TRY(cudaGetLastError());
             if (int rc = take_enqueue_error()) return rc;
@@ -1197,6 +1201,8 @@ class Server {
                 std::lock_guard<std::mutex> lk(mu_);
                 if (status == fomo::kErrTmaTimeout)
                     finish_locked(r, kFailed, FOMO_ETIMEOUT, "a TMA load of a batch time-step kernel did not complete");
+                else if (status == fomo::kErrBatchParity)
+                    finish_locked(r, kFailed, FOMO_ECUDA, "a batch launch's step parity disagreed with its step counter");
                 else if (status)
                     finish_locked(r, kFailed, FOMO_ECUDA, "batch time-step kernel reported error " + std::to_string(status));
                 else

@@ -58,6 +58,7 @@ struct GroupDev {
 struct BatchHead {
     const int* step;                  // batch step (1-based) of the launch's half step
     int* advance;                     // the other half step's counter of the set (block 0 advances it)
+    int kpar;                         // parity of that batch step (the host knows it when it launches)
     int n_shots, n_groups;
     int total_band, total_tile;
     int rec_off[kShotsPerLaunch + 1]; // first receiver block of each shot
@@ -140,6 +141,12 @@ __device__ __forceinline__ int local_step(const BatchHead& H, const BatchShot& S
     return *H.step - S.start + 1;
 }
 
+// The wavefield copy a shot's step reads, (ks - 1) & 1, from the launch's
+// step parity alone: no memory access stands between a tile block's start
+// and its TMA loads.  A block whose local step disagrees flags an error.
+__device__ __forceinline__ int read_copy(const BatchHead& H, const BatchShot& S) { return (H.kpar ^ S.start) & 1; }
+constexpr int kErrBatchParity = 3;
+
 __device__ __forceinline__ float wavelet_at(const BatchShot& S, int ks) {
     return (ks >= 1 && ks <= S.n_wavelet) ? __ldg(S.wavelet + ks - 1) : 0.f;
 }
@@ -171,25 +178,29 @@ __global__ void __launch_bounds__(kThreads, kTileBlocks<M>) batch_velocity_kerne
     if (it.role < 0) return;
     const BatchShot& S = L.shot[it.shot];
     const int ks = local_step(L.H, S);
-    const int a = (ks - 1) & 1;
     if (it.role == 2) {
+        const int a = (ks - 1) & 1;
         grid_dep_wait();  // receivers may sit in the band rows
         if (ks >= 2 && ks <= S.nt + 1) record_block(S.P[a], it.local, ks - 1);  // state after step ks-1: copy a
         return;
     }
-    if (ks < 1 || ks > S.nt) return;
-    const float src_w = wavelet_at(S, ks);
-    const StepParams& P = S.P[a];
+    // the tile path: the copy from the launch's parity, the step's range
+    // checked once the boxes are on their way (live)
+    const int c = read_copy(L.H, S);
+    const bool live = ks >= 1 && ks <= S.nt;
+    const StepParams& P = S.P[c];
     const TileKind k = classify(P, S.T, it.local);
     if (reads_band_rows(P, k.z0)) grid_dep_wait();
     if (k.generic) {
-        edge_tile<M, true>(P, S.T, k.x0, k.z0, k.x_end, smem, src_w);
+        if (!live) return;
+        edge_tile<M, true>(P, S.T, k.x0, k.z0, k.x_end, smem, wavelet_at(S, ks));
     } else {
         const int s = it.shot;
-        const VelMapRefs mp{&L.tau[s][a][0], &L.tau[s][a][1], &L.tau[s][a][2], &L.v[s][a][0], &L.v[s][a][1],
+        const VelMapRefs mp{&L.tau[s][c][0], &L.tau[s][c][1], &L.tau[s][c][2], &L.v[s][c][0], &L.v[s][c][1],
                             &L.b[s][0],      &L.b[s][1],      &L.b[s][2],      &L.b[s][3]};
-        fast_vel<M>(P, S.T, mp, k.x0, k.z0, k.x_end, k.band, k.rim, smem, src_w);
+        fast_vel<M>(P, S.T, mp, k.x0, k.z0, k.x_end, k.band, k.rim, smem, wavelet_at(S, ks), -1, live);
     }
+    if (threadIdx.x == 0 && live && ((ks - 1) & 1) != c) atomicCAS(S.T.status, 0, kErrBatchParity);
 }
 
 template <int M>
@@ -200,20 +211,21 @@ __global__ void __launch_bounds__(kThreads, kTileBlocks<M>) batch_stress_kernel(
     if (it.role < 0) return;
     const BatchShot& S = L.shot[it.shot];
     const int ks = local_step(L.H, S);
-    if (ks < 1 || ks > S.nt) return;
-    const int a = (ks - 1) & 1, b = 1 - a;
-    const float src_w = wavelet_at(S, ks);
+    const int a = read_copy(L.H, S), b = 1 - a;  // as in the velocity launch
+    const bool live = ks >= 1 && ks <= S.nt;
     const StepParams& P = S.P[a];
     const TileKind k = classify(P, S.T, it.local);
     if (reads_band_rows(P, k.z0)) grid_dep_wait();
     if (k.generic) {
-        edge_tile<M, false>(P, S.T, k.x0, k.z0, k.x_end, smem, src_w);
+        if (!live) return;
+        edge_tile<M, false>(P, S.T, k.x0, k.z0, k.x_end, smem, wavelet_at(S, ks));
     } else {
         const int s = it.shot;
         const StrMapRefs mp{&L.v[s][b][0],   &L.v[s][b][1],   &L.tau[s][a][0], &L.tau[s][a][1],
                             &L.tau[s][a][2], &L.mod[s][0],    &L.mod[s][1],    &L.mod[s][2]};
-        fast_str<M>(P, S.T, mp, k.x0, k.z0, k.x_end, k.band, k.rim, smem, src_w);
+        fast_str<M>(P, S.T, mp, k.x0, k.z0, k.x_end, k.band, k.rim, smem, wavelet_at(S, ks), -1, live);
     }
+    if (threadIdx.x == 0 && live && ((ks - 1) & 1) != a) atomicCAS(S.T.status, 0, kErrBatchParity);
 }
 
 // Band pass of every shot in flight (after the tile launch of the same half

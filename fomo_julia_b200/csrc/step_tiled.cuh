@@ -437,9 +437,12 @@ __device__ void prefetch_vel(const StepParams& P, const TiledArgs& T, const VelM
 template <int M>
 __device__ void prefetch_str(const StepParams& P, const TiledArgs& T, const StrMapRefs& mp, int tile);
 
+// live == false (a batched shot outside its step range, known only after the
+// copies were started): the block waits for its boxes and stores nothing.
 template <int M>
 __device__ __forceinline__ void fast_vel(const StepParams& P, const TiledArgs& T, const VelMapRefs& mp, int x0, int z0,
-                                         int x_end, bool band, bool rim, float* smem, float src_w, int pf_tile = -1) {
+                                         int x_end, bool band, bool rim, float* smem, float src_w, int pf_tile = -1,
+                                         bool live = true) {
     using G = Geo<M>;
     constexpr int BOX = G::BOXS;
     float* s_xx = smem;
@@ -477,6 +480,10 @@ __device__ __forceinline__ void fast_vel(const StepParams& P, const TiledArgs& T
     }
     __syncthreads();
     if (!wait_tma(bar, T)) return;
+    if (!live) {  // every copy of the block lands before it leaves
+        wait_tma(bar + 1, T);
+        return;
+    }
     // The source, added to the stresses read: only the block whose halo box
     // holds it needs a block barrier (the condition is block-uniform; every
     // other thread sees the boxes through its own wait on bar[0]).
@@ -567,7 +574,8 @@ __device__ __forceinline__ void fast_vel(const StepParams& P, const TiledArgs& T
 
 template <int M>
 __device__ __forceinline__ void fast_str(const StepParams& P, const TiledArgs& T, const StrMapRefs& mp, int x0, int z0,
-                                         int x_end, bool band, bool rim, float* smem, float src_w, int pf_tile = -1) {
+                                         int x_end, bool band, bool rim, float* smem, float src_w, int pf_tile = -1,
+                                         bool live = true) {
     using G = Geo<M>;
     constexpr int BOX = G::BOXS;
     float* s_vx = smem;
@@ -598,6 +606,10 @@ __device__ __forceinline__ void fast_str(const StepParams& P, const TiledArgs& T
     }
     __syncthreads();
     if (!wait_tma(bar, T)) return;
+    if (!live) {  // every copy of the block lands before it leaves
+        wait_tma(bar + 1, T);
+        return;
+    }
 
     const int cg = threadIdx.x % kCG, rp = threadIdx.x / kCG;
     const int x = x0 + 4 * cg, zt = z0 + 2 * rp;

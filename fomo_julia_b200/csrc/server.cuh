@@ -836,6 +836,7 @@ class Server {
             H.advance = cnt + 1;
             H.n_shots = (int)(j - i);
             H.n_groups = n_groups;
+            H.pf_ahead = fomo::prefetch_distance(sm_count());
             H.total_band = band;
             H.total_tile = tile;
             S.ls->H = H;

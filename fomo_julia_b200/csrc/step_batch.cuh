@@ -59,6 +59,7 @@ struct BatchHead {
     const int* step;                  // batch step (1-based) of the launch's half step
     int* advance;                     // the other half step's counter of the set (block 0 advances it)
     int kpar;                         // parity of that batch step (the host knows it when it launches)
+    int pf_ahead;                     // tile blocks between a block and the one whose boxes it prefetches
     int n_shots, n_groups;
     int total_band, total_tile;
     int rec_off[kShotsPerLaunch + 1]; // first receiver block of each shot
@@ -170,6 +171,43 @@ __global__ void batch_counters_kernel(int* counters, int n, int step) {
     }
 }
 
+// L2 prefetch of the boxes of tile block `b` of a launch (thread 0, right
+// after its own tile's copies): the shot's own boxes, and the medium boxes
+// only for the group's first shot (its other shots read the same ones).
+// The copy comes from the launch's parity, so nothing is loaded first.
+template <int M, bool VEL, class LaunchT>
+struct BatchPrefetch {
+    const LaunchT& L;
+    int b;
+    __device__ void operator()() const {
+        const BatchHead& H = L.H;
+        if (b >= H.total_tile) return;
+        const BatchItem it = in_groups<true>(H, b);
+        const BatchShot& S = L.shot[it.shot];
+        if (it.local >= S.T.n_tile_blocks) return;
+        const TileKind k = classify(S.P[0], S.T, it.local);
+        if (k.generic) return;
+        int g = 0;
+#pragma unroll 1
+        for (int h = 1; h < H.n_groups; ++h)
+            if (H.groups[h].tile_off <= b) g = h;
+        const bool medium = it.shot == H.groups[g].first;
+        const int s = it.shot, c = read_copy(H, S);
+        using G = Geo<M>;
+        if constexpr (VEL) {
+            for (int f = 0; f < 3; ++f) tma_prefetch_2d(&L.tau[s][c][f], k.x0 - G::HX, k.z0 - M);
+            for (int f = 0; f < 2; ++f) tma_prefetch_2d(&L.v[s][c][f], k.x0, k.z0);
+            if (medium)
+                for (int q = 0; q < (S.T.iso ? 3 : 4); q += (S.T.iso ? 2 : 1)) tma_prefetch_2d(&L.b[s][q], k.x0, k.z0);
+        } else {
+            for (int f = 0; f < 2; ++f) tma_prefetch_2d(&L.v[s][1 - c][f], k.x0 - G::HX, k.z0 - M);
+            for (int f = 0; f < 3; ++f) tma_prefetch_2d(&L.tau[s][c][f], k.x0, k.z0);
+            if (medium)
+                for (int q = 0; q < 3; ++q) tma_prefetch_2d(&L.mod[s][q], k.x0, k.z0);
+        }
+    }
+};
+
 template <int M>
 __global__ void __launch_bounds__(kThreads, kTileBlocks<M>) batch_velocity_kernel(const __grid_constant__ BatchVelLaunch L) {
     extern __shared__ __align__(128) float smem[];
@@ -198,7 +236,8 @@ __global__ void __launch_bounds__(kThreads, kTileBlocks<M>) batch_velocity_kerne
         const int s = it.shot;
         const VelMapRefs mp{&L.tau[s][c][0], &L.tau[s][c][1], &L.tau[s][c][2], &L.v[s][c][0], &L.v[s][c][1],
                             &L.b[s][0],      &L.b[s][1],      &L.b[s][2],      &L.b[s][3]};
-        fast_vel<M>(P, S.T, mp, k.x0, k.z0, k.x_end, k.band, k.rim, smem, wavelet_at(S, ks), -1, live);
+        const BatchPrefetch<M, true, BatchVelLaunch> pf{L, L.H.pf_ahead > 0 ? (int)blockIdx.x + L.H.pf_ahead : 1 << 30};
+        fast_vel<M>(P, S.T, mp, k.x0, k.z0, k.x_end, k.band, k.rim, smem, wavelet_at(S, ks), -1, live, pf);
     }
     if (threadIdx.x == 0 && live && ((ks - 1) & 1) != c) atomicCAS(S.T.status, 0, kErrBatchParity);
 }
@@ -223,7 +262,8 @@ __global__ void __launch_bounds__(kThreads, kTileBlocks<M>) batch_stress_kernel(
         const int s = it.shot;
         const StrMapRefs mp{&L.v[s][b][0],   &L.v[s][b][1],   &L.tau[s][a][0], &L.tau[s][a][1],
                             &L.tau[s][a][2], &L.mod[s][0],    &L.mod[s][1],    &L.mod[s][2]};
-        fast_str<M>(P, S.T, mp, k.x0, k.z0, k.x_end, k.band, k.rim, smem, wavelet_at(S, ks), -1, live);
+        const BatchPrefetch<M, false, BatchStrLaunch> pf{L, L.H.pf_ahead > 0 ? (int)blockIdx.x + L.H.pf_ahead : 1 << 30};
+        fast_str<M>(P, S.T, mp, k.x0, k.z0, k.x_end, k.band, k.rim, smem, wavelet_at(S, ks), -1, live, pf);
     }
     if (threadIdx.x == 0 && live && ((ks - 1) & 1) != a) atomicCAS(S.T.status, 0, kErrBatchParity);
 }

@@ -437,12 +437,18 @@ __device__ void prefetch_vel(const StepParams& P, const TiledArgs& T, const VelM
 template <int M>
 __device__ void prefetch_str(const StepParams& P, const TiledArgs& T, const StrMapRefs& mp, int tile);
 
+// A call thread 0 makes right after starting a tile's copies (the batched
+// launches' L2 prefetch of a later block); none by default.
+struct NoHook {
+    __device__ void operator()() const {}
+};
+
 // live == false (a batched shot outside its step range, known only after the
 // copies were started): the block waits for its boxes and stores nothing.
-template <int M>
+template <int M, class Hook = NoHook>
 __device__ __forceinline__ void fast_vel(const StepParams& P, const TiledArgs& T, const VelMapRefs& mp, int x0, int z0,
                                          int x_end, bool band, bool rim, float* smem, float src_w, int pf_tile = -1,
-                                         bool live = true) {
+                                         bool live = true, const Hook& hook = Hook()) {
     using G = Geo<M>;
     constexpr int BOX = G::BOXS;
     float* s_xx = smem;
@@ -477,6 +483,7 @@ __device__ __forceinline__ void fast_vel(const StepParams& P, const TiledArgs& T
             tma_load_2d(p_b3, mp.b3, x0, z0, bar + 1);
         }
         if (pf_tile >= 0) prefetch_vel<M>(P, T, mp, pf_tile);
+        hook();
     }
     __syncthreads();
     if (!wait_tma(bar, T)) return;
@@ -572,10 +579,10 @@ __device__ __forceinline__ void fast_vel(const StepParams& P, const TiledArgs& T
     }
 }
 
-template <int M>
+template <int M, class Hook = NoHook>
 __device__ __forceinline__ void fast_str(const StepParams& P, const TiledArgs& T, const StrMapRefs& mp, int x0, int z0,
                                          int x_end, bool band, bool rim, float* smem, float src_w, int pf_tile = -1,
-                                         bool live = true) {
+                                         bool live = true, const Hook& hook = Hook()) {
     using G = Geo<M>;
     constexpr int BOX = G::BOXS;
     float* s_vx = smem;
@@ -603,6 +610,7 @@ __device__ __forceinline__ void fast_str(const StepParams& P, const TiledArgs& T
         tma_load_2d(p_mu, mp.mu, x0, z0, bar + 1);
         tma_load_2d(p_mxz, mp.mxz, x0, z0, bar + 1);
         if (pf_tile >= 0) prefetch_str<M>(P, T, mp, pf_tile);
+        hook();
     }
     __syncthreads();
     if (!wait_tma(bar, T)) return;

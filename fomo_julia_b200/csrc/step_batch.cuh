@@ -31,8 +31,12 @@
 // Inside a group, tile and band blocks are interleaved tile-major
 // (block = local * n + shot), so the n shots' copies of one tile run side by
 // side and the medium tile is read from HBM once and from L2 by the others.
-// A block whose shot is outside its step range returns at once; that is how
-// shots join and leave a running batch at step boundaries.
+// A tile block takes its shot's wavefield copy from the launch's step parity
+// (BatchHead::kpar), so its TMA loads start at once, and reads the step
+// counter beside them; a block whose shot is outside its step range stores
+// nothing (receiver and generic-tile blocks return at once).  That is how
+// shots join and leave a running batch at step boundaries.  Thread 0 of a
+// fast tile also prefetches into L2 the boxes of the block pf_ahead later.
 //
 // Every block runs the single-shot code (edge_tile, fast_vel, fast_str,
 // record_block, band_march) on its shot's parameters, so a batched shot's

@@ -50,7 +50,7 @@ def parse():
     p.add_argument("--no-batched", action="store_true", help="skip the batched-shots section")
     p.add_argument("--no-serving", action="store_true", help="skip the serving section")
     p.add_argument("--batch-nt", type=int, default=None, help="override nt of the batched section (development)")
-    p.add_argument("--serve-requests", type=int, default=200,
+    p.add_argument("--serve-requests", type=int, default=400,
                    help="requests of the serving sample (the full stream of the serving workload is 2000)")
     p.add_argument("--serve-load", type=float, default=4.0,
                    help="offered load of the serving sample, as a multiple of the sequential plain capacity")

@@ -7,6 +7,7 @@ other media, other FD orders, shots joining and leaving mid-run).  The single
 path itself is checked against the oracle in test_gpu_parity.py; one batched
 shot is also checked against the oracle directly here.
 """
+import dataclasses
 import time
 from dataclasses import dataclass
 
@@ -110,6 +111,24 @@ def test_steps_per_launch_do_not_change_results(b200, K):
     for r, g in zip(out, refs):
         assert np.array_equal(r.gather, g)
     assert st["completed"] == 3 and st["failed"] == 0
+    S.med.release()
+
+
+def test_batch_with_dz_not_dx(b200):
+    """dz != dx: four buoyancy arrays per medium (the tiles load and prefetch
+    all four); a batch of three shots equals the shots run alone."""
+    c = dataclasses.replace(layered(**MEDIUM_A), dz=13.0)
+    S = setup(c, b200)
+    xs = source_xs(c, 3)
+    nts = [100, 61, 80]
+    refs = [single(S, source(S, x, 26.0, nt), b200, nt) for x, nt in zip(xs, nts)]
+    with F.ShotServer(steps_per_launch=8) as srv:
+        ts = [srv.submit(S.med, S.H, S.a, source(S, x, 26.0, nt), S.rec, params_of(S, nt), shot_id=i)
+              for i, (x, nt) in enumerate(zip(xs, nts))]
+        out = [srv.wait(t, timeout=WAIT_S) for t in ts]
+    for r, g in zip(out, refs):
+        assert np.array_equal(r.gather, g)
+    assert max(r.stats["batch_peak"] for r in out) >= 2
     S.med.release()
 
 
